@@ -1,0 +1,146 @@
+/*
+ * zkgpu.h — C ABI of libzkgpu.so, the B200 (sm_100a) implementation of the
+ * halo2/BN256 prover hot path: the Fr NTT (forward, inverse, coset /
+ * extended-domain LDE) and the G1 Pippenger MSM.
+ *
+ * Data layout (all entry points): one field element = 4 x uint64_t little
+ * endian limbs in Montgomery form (R = 2^256), canonical (< modulus) — the
+ * layout of the reference's BigNum (cuda/bn256.h:10-13) and of halo2curves'
+ * Fr / Fq.  Affine points are {x, y} with the identity encoded as (0, 0);
+ * projective points are Jacobian {X, Y, Z} (x = X/Z^2, y = Y/Z^3) with the
+ * identity Z = 0 (cuda/bn256.h:15-28, src/lib.rs:22-35).
+ *
+ * Status convention: 0 = success, otherwise a ZKGPU_E* code below.  No entry
+ * point prints, exits or aborts the host process (the reference exit()s on
+ * CUDA errors, cuda/fft.cu:380-395).
+ */
+#ifndef ZKGPU_H
+#define ZKGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* src/lib.rs:22-28 (#[repr(C)] GpuAffine) */
+typedef struct {
+    uint64_t x[4];
+    uint64_t y[4];
+} GpuAffine;
+
+/* src/lib.rs:30-35 (#[repr(C)] GpuProjective) */
+typedef struct {
+    uint64_t x[4];
+    uint64_t y[4];
+    uint64_t z[4];
+} GpuProjective;
+
+enum {
+    ZKGPU_OK = 0,
+    ZKGPU_EINVAL = 1,    /* bad size, null pointer, omega not of order n, ... */
+    ZKGPU_ENOMEM = 2,    /* device allocation failed */
+    ZKGPU_ECUDA = 3,     /* CUDA runtime error (message: zkgpu_last_error) */
+    ZKGPU_ETIMEOUT = 4,  /* a bounded device wait expired */
+    ZKGPU_EADMIT = 5,    /* serving: job larger than the HBM budget */
+    ZKGPU_ENODEV = 6,    /* no such CUDA device */
+    ZKGPU_EBUSY = 7      /* serving: queue full / shut down */
+};
+
+/* ======================================================================
+ * Reference-compatible entry points.  Signatures are the Rust declarations
+ * of src/api.rs:3-14 (usize -> size_t, u64 -> uint64_t); they are
+ * synchronous and operate on caller-owned HOST buffers, like the C
+ * definitions they replace (cuda/fft.cu:553-583).
+ * ====================================================================== */
+
+/* src/api.rs:4 / cuda/fft.cu:554-558: device self-test.  Runs a field
+ * known-answer check on `device_id`; returns 0 on success. */
+uint64_t do_fft_ffi(size_t device_id);
+
+/* src/api.rs:6 / cuda/fft.cu:560-564: in-place forward NTT of `req`
+ * (n = 2^log_n elements, natural order in and out) with root `omega`.
+ * `twiddle` / `twiddle_size` (halo2 generate_twiddle_lookup_table(omega,
+ * log_n, 10, true)) are accepted for ABI compatibility; the device derives
+ * its own tables from `omega`, which must have order exactly n. */
+uint64_t parallel_fft_api(size_t device_id, uint64_t *req, const uint64_t *omega, const uint64_t *twiddle,
+                          uint64_t n, uint64_t log_n, uint64_t twiddle_size);
+
+/* src/api.rs:8 / cuda/fft.cu:566-570: in-place inverse NTT: forward NTT
+ * with `omega` (the caller passes w^-1) then every element * `divisor`
+ * (the caller passes n^-1). */
+uint64_t parallel_ifft_api(size_t device_id, uint64_t *req, const uint64_t *omega, const uint64_t *twiddle,
+                           uint64_t n, uint64_t log_n, uint64_t twiddle_size, const uint64_t *divisor);
+
+/* src/api.rs:10 / cuda/fft.cu:572-576, :223-232: req[i] *= c^i, then the
+ * forward NTT (one part of the extended-domain evaluation). */
+uint64_t parallel_coeff_to_extended_part_api(size_t device_id, uint64_t *req, const uint64_t *omega,
+                                             const uint64_t *twiddle, uint64_t n, uint64_t log_n,
+                                             uint64_t twiddle_size, const uint64_t *c);
+
+/* src/api.rs:12 / cuda/fft.cu:578-582, :450-551: acc = sum_i data[i] *
+ * bases[i] (data: Fr Montgomery scalars, bases: affine Fq Montgomery).
+ * Any length >= 0 (the reference needs a power of two > 256).  The result
+ * is written normalised: Z = Montgomery one, or all-zero for the identity. */
+uint64_t parallel_msm_api(size_t device_id, const uint64_t *data, const GpuAffine *bases, uint64_t lenght,
+                          GpuProjective *acc);
+
+/* ======================================================================
+ * Host-buffer API with the north-star names (fft / ifft / coset_fft / msm).
+ * ====================================================================== */
+int zkgpu_fft(int device, uint64_t *a, uint32_t log_n, const uint64_t omega[4]);
+int zkgpu_ifft(int device, uint64_t *a, uint32_t log_n, const uint64_t omega_inv[4], const uint64_t divisor[4]);
+int zkgpu_coset_fft(int device, uint64_t *a, uint32_t log_n, const uint64_t omega[4], const uint64_t c[4]);
+int zkgpu_msm(int device, const uint64_t *scalars, const uint64_t *bases_xy, uint64_t n, uint64_t out_xyz[12]);
+
+/* halo2 coset LDE as one call (lagrange -> extended):
+ *   coeffs = ifft(values, omega_inv, n^-1);  coeffs[i] *= g^i;
+ *   ext    = fft(zero-pad(coeffs, 2^log_ext), omega_ext)      (natural order)
+ * values: 2^log_n host elements (read only); ext: 2^log_ext host elements. */
+int zkgpu_lagrange_to_extended(int device, const uint64_t *values, uint32_t log_n, uint64_t *ext, uint32_t log_ext,
+                               const uint64_t omega_inv[4], const uint64_t divisor[4], const uint64_t g[4],
+                               const uint64_t omega_ext[4]);
+
+/* ======================================================================
+ * Device-resident API: pointers are device memory on `device`, work is
+ * enqueued on `stream` (a cudaStream_t, NULL = legacy default) and the call
+ * returns without synchronising.  Scratch comes from the stream's pool.
+ * ====================================================================== */
+/* in place; optional coset (a[i] *= c^i first) and post scale (every output * scale) */
+int zkgpu_ntt_dev(int device, uint64_t *d_a, uint32_t log_n, const uint64_t omega[4], const uint64_t *coset_c,
+                  const uint64_t *post_scale, void *stream);
+/* d_values (2^log_n) -> d_ext (2^log_ext), the same pipeline as
+ * zkgpu_lagrange_to_extended; d_values is not modified. */
+int zkgpu_lagrange_to_extended_dev(int device, const uint64_t *d_values, uint32_t log_n, uint64_t *d_ext,
+                                   uint32_t log_ext, const uint64_t omega_inv[4], const uint64_t divisor[4],
+                                   const uint64_t g[4], const uint64_t omega_ext[4], void *stream);
+/* d_out_xyz receives the Jacobian sum (12 words, device memory) */
+int zkgpu_msm_dev(int device, const uint64_t *d_scalars, const uint64_t *d_bases_xy, uint64_t n, uint64_t *d_out_xyz,
+                  void *stream);
+
+/* ======================================================================
+ * Diagnostics.
+ * ====================================================================== */
+/* elementwise field op on host arrays through the device kernels:
+ * op 0 = mul, 1 = add, 2 = sub;  fid 0 = Fr, 1 = Fq */
+int zkgpu_field_op(int device, int op, int fid, const uint64_t *a, const uint64_t *b, uint64_t *out, uint64_t n);
+/* message of the last ZKGPU_ECUDA on this thread ("" if none) */
+const char *zkgpu_last_error(void);
+/* kernel launches issued by this thread since the last reset */
+uint64_t zkgpu_launch_count(int reset);
+/* library version string */
+const char *zkgpu_version(void);
+/* measured 32-bit integer multiply-add issue rate of `device` (IMAD/s) and
+ * the rate of this library's Fr Montgomery product (products/s) */
+int zkgpu_int_peak(int device, uint32_t iters, double *imad_per_s, double *modmul_per_s);
+/* opt-in CUDA-event timing of each kernel launch, per kernel name */
+void zkgpu_prof_enable(int on);
+void zkgpu_prof_reset(void);
+/* lines "name launches total_ms work_modmul bytes"; returns the line count */
+int zkgpu_prof_read(char *buf, uint64_t cap);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ZKGPU_H */

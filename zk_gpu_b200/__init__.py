@@ -1,0 +1,258 @@
+"""zk_gpu_b200 — B200 (sm_100a) halo2/BN256 NTT + MSM behind a C ABI.
+
+The product is ``libzkgpu.so`` (CUDA kernels + C-ABI, ``include/zkgpu.h``).
+This module is the Python host mirror of the reference's FFI surface
+(src/api.rs:3-14): the same entry-point names, argument meaning and status
+codes, over ``ctypes``.  Arrays are numpy ``uint64`` with a trailing
+dimension of 4 (one Fr/Fq element, 4 x u64 little-endian Montgomery limbs)
+or 8 (one affine G1 point x, y).  Device-resident variants take torch CUDA
+tensors (``torch.uint64`` / ``int64`` storage) and a CUDA stream.
+
+There is no CPU fallback: if the library is missing, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libzkgpu.so")
+
+OK, EINVAL, ENOMEM, ECUDA, ETIMEOUT, EADMIT, ENODEV, EBUSY = range(8)
+_STATUS = {0: "OK", 1: "EINVAL", 2: "ENOMEM", 3: "ECUDA", 4: "ETIMEOUT", 5: "EADMIT", 6: "ENODEV", 7: "EBUSY"}
+
+_lib = None
+
+
+class ZkGpuError(RuntimeError):
+    def __init__(self, code: int, where: str = ""):
+        msg = _STATUS.get(int(code), str(code))
+        detail = ""
+        try:
+            detail = lib().zkgpu_last_error().decode()
+        except Exception:  # pragma: no cover
+            pass
+        super().__init__(f"{where}: {msg} {detail}".strip())
+        self.code = int(code)
+
+
+class GpuAffine(ctypes.Structure):
+    """src/lib.rs:22-28"""
+    _fields_ = [("x", ctypes.c_uint64 * 4), ("y", ctypes.c_uint64 * 4)]
+
+
+class GpuProjective(ctypes.Structure):
+    """src/lib.rs:30-35"""
+    _fields_ = [("x", ctypes.c_uint64 * 4), ("y", ctypes.c_uint64 * 4), ("z", ctypes.c_uint64 * 4)]
+
+
+# name -> (restype, argtypes); exactly the functions include/zkgpu.h declares
+P = ctypes.c_void_p
+_u64, _u32, _i32, _sz = ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int, ctypes.c_size_t
+EXPORTS = {
+    "do_fft_ffi": (_u64, [_sz]),
+    "parallel_fft_api": (_u64, [_sz, P, P, P, _u64, _u64, _u64]),
+    "parallel_ifft_api": (_u64, [_sz, P, P, P, _u64, _u64, _u64, P]),
+    "parallel_coeff_to_extended_part_api": (_u64, [_sz, P, P, P, _u64, _u64, _u64, P]),
+    "parallel_msm_api": (_u64, [_sz, P, P, _u64, P]),
+    "zkgpu_fft": (_i32, [_i32, P, _u32, P]),
+    "zkgpu_ifft": (_i32, [_i32, P, _u32, P, P]),
+    "zkgpu_coset_fft": (_i32, [_i32, P, _u32, P, P]),
+    "zkgpu_msm": (_i32, [_i32, P, P, _u64, P]),
+    "zkgpu_lagrange_to_extended": (_i32, [_i32, P, _u32, P, _u32, P, P, P, P]),
+    "zkgpu_ntt_dev": (_i32, [_i32, P, _u32, P, P, P, P]),
+    "zkgpu_lagrange_to_extended_dev": (_i32, [_i32, P, _u32, P, _u32, P, P, P, P, P]),
+    "zkgpu_msm_dev": (_i32, [_i32, P, P, _u64, P, P]),
+    "zkgpu_field_op": (_i32, [_i32, _i32, _i32, P, P, P, _u64]),
+    "zkgpu_last_error": (ctypes.c_char_p, []),
+    "zkgpu_launch_count": (_u64, [_i32]),
+    "zkgpu_version": (ctypes.c_char_p, []),
+    "zkgpu_int_peak": (_i32, [_i32, _u32, P, P]),
+    "zkgpu_prof_enable": (None, [_i32]),
+    "zkgpu_prof_reset": (None, []),
+    "zkgpu_prof_read": (_i32, [ctypes.c_char_p, _u64]),
+}
+
+
+def lib():
+    """Load libzkgpu.so (built in-tree by zk_gpu_b200.build)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run `python -m zk_gpu_b200.build` (no CPU fallback exists)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in EXPORTS.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _arr(a, words=4) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.uint64)
+    assert a.ndim >= 1 and a.shape[-1] == words, f"expected trailing dimension {words}"
+    return a
+
+
+def _el(x) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(x, dtype=np.uint64).reshape(4))
+
+
+def _check(code: int, where: str):
+    if int(code) != 0:
+        raise ZkGpuError(int(code), where)
+
+
+# ---------------------------------------------------------------------------
+# reference-compatible entry points (src/api.rs:3-14), raw status returned
+# ---------------------------------------------------------------------------
+def do_fft_ffi(device_id: int = 0) -> int:
+    return int(lib().do_fft_ffi(device_id))
+
+
+def parallel_fft_api(device_id: int, req: np.ndarray, omega, twiddle, n: int, log_n: int, twiddle_size: int) -> int:
+    """In place on ``req`` ((n, 4) uint64, C-contiguous)."""
+    tw = None if twiddle is None else _arr(twiddle).ctypes.data
+    return int(lib().parallel_fft_api(device_id, req.ctypes.data, _el(omega).ctypes.data, tw, n, log_n, twiddle_size))
+
+
+def parallel_ifft_api(device_id: int, req: np.ndarray, omega, twiddle, n: int, log_n: int, twiddle_size: int,
+                      divisor) -> int:
+    tw = None if twiddle is None else _arr(twiddle).ctypes.data
+    return int(lib().parallel_ifft_api(device_id, req.ctypes.data, _el(omega).ctypes.data, tw, n, log_n,
+                                       twiddle_size, _el(divisor).ctypes.data))
+
+
+def parallel_coeff_to_extended_part_api(device_id: int, req: np.ndarray, omega, twiddle, n: int, log_n: int,
+                                        twiddle_size: int, c) -> int:
+    tw = None if twiddle is None else _arr(twiddle).ctypes.data
+    return int(lib().parallel_coeff_to_extended_part_api(device_id, req.ctypes.data, _el(omega).ctypes.data, tw, n,
+                                                         log_n, twiddle_size, _el(c).ctypes.data))
+
+
+def parallel_msm_api(device_id: int, data: np.ndarray, bases: np.ndarray, length: int, acc: GpuProjective) -> int:
+    return int(lib().parallel_msm_api(device_id, _arr(data).ctypes.data, _arr(bases, 8).ctypes.data, length,
+                                      ctypes.addressof(acc)))
+
+
+# ---------------------------------------------------------------------------
+# north-star names: fft / ifft / coset_fft / msm (return new arrays, raise)
+# ---------------------------------------------------------------------------
+def fft(a: np.ndarray, omega, log_n: int, device: int = 0) -> np.ndarray:
+    out = np.array(_arr(a), copy=True)
+    _check(lib().zkgpu_fft(device, out.ctypes.data, log_n, _el(omega).ctypes.data), "fft")
+    return out
+
+
+def ifft(a: np.ndarray, omega_inv, log_n: int, divisor, device: int = 0) -> np.ndarray:
+    out = np.array(_arr(a), copy=True)
+    _check(lib().zkgpu_ifft(device, out.ctypes.data, log_n, _el(omega_inv).ctypes.data, _el(divisor).ctypes.data),
+           "ifft")
+    return out
+
+
+def coset_fft(a: np.ndarray, omega, log_n: int, c, device: int = 0) -> np.ndarray:
+    out = np.array(_arr(a), copy=True)
+    _check(lib().zkgpu_coset_fft(device, out.ctypes.data, log_n, _el(omega).ctypes.data, _el(c).ctypes.data),
+           "coset_fft")
+    return out
+
+
+def lagrange_to_extended(values: np.ndarray, log_n: int, log_ext: int, omega_inv, divisor, g, omega_ext,
+                         device: int = 0) -> np.ndarray:
+    v = _arr(values)
+    ext = np.empty((1 << log_ext, 4), np.uint64)
+    _check(lib().zkgpu_lagrange_to_extended(device, v.ctypes.data, log_n, ext.ctypes.data, log_ext,
+                                            _el(omega_inv).ctypes.data, _el(divisor).ctypes.data,
+                                            _el(g).ctypes.data, _el(omega_ext).ctypes.data), "lagrange_to_extended")
+    return ext
+
+
+def msm(scalars: np.ndarray, bases: np.ndarray, device: int = 0) -> np.ndarray:
+    """Returns the Jacobian sum (12 u64: X, Y, Z), normalised (Z = one) or all-zero."""
+    s, b = _arr(scalars), _arr(bases, 8)
+    assert s.shape[0] == b.shape[0]
+    out = np.zeros(12, np.uint64)
+    _check(lib().zkgpu_msm(device, s.ctypes.data, b.ctypes.data, s.shape[0], out.ctypes.data), "msm")
+    return out
+
+
+def field_op(op: str, a: np.ndarray, b: np.ndarray, field: str = "fr", device: int = 0) -> np.ndarray:
+    a, b = _arr(a), _arr(b)
+    out = np.empty_like(a)
+    _check(lib().zkgpu_field_op(device, {"mul": 0, "add": 1, "sub": 2}[op], {"fr": 0, "fq": 1}[field],
+                                a.ctypes.data, b.ctypes.data, out.ctypes.data, a.shape[0]), "field_op")
+    return out
+
+
+def launch_count(reset: bool = False) -> int:
+    return int(lib().zkgpu_launch_count(1 if reset else 0))
+
+
+def int_peak(device: int = 0, iters: int = 4096):
+    """(IMAD/s, Fr Montgomery products/s) measured on `device`."""
+    a, b = ctypes.c_double(), ctypes.c_double()
+    _check(lib().zkgpu_int_peak(device, iters, ctypes.byref(a), ctypes.byref(b)), "int_peak")
+    return a.value, b.value
+
+
+def prof_enable(on: bool = True):
+    lib().zkgpu_prof_enable(1 if on else 0)
+
+
+def prof_reset():
+    lib().zkgpu_prof_reset()
+
+
+def prof_read() -> dict:
+    """{kernel: {"launches", "ms", "work", "bytes"}} for launches timed since the last reset."""
+    buf = ctypes.create_string_buffer(1 << 16)
+    lib().zkgpu_prof_read(buf, len(buf))
+    out = {}
+    for line in buf.value.decode().splitlines():
+        name, cnt, ms, work, by = line.split()
+        out[name] = {"launches": int(cnt), "ms": float(ms), "work": float(work), "bytes": float(by)}
+    return out
+
+
+# ---------------------------------------------------------------------------
+# device-resident API over torch tensors (plumbing only)
+# ---------------------------------------------------------------------------
+def _ptr(t) -> int:
+    return int(t.data_ptr())
+
+
+def _stream_ptr(stream) -> int | None:
+    if stream is None:
+        import torch
+        return int(torch.cuda.current_stream().cuda_stream)
+    return int(getattr(stream, "cuda_stream", stream))
+
+
+def ntt_dev(t, log_n: int, omega, coset=None, post_scale=None, stream=None, device: int | None = None):
+    """In-place NTT of a CUDA tensor of shape (2^log_n, 4), dtype int64/uint64."""
+    dev = t.device.index if device is None else device
+    c = _el(coset).ctypes.data if coset is not None else None
+    cc = _el(coset) if coset is not None else None
+    ps = _el(post_scale) if post_scale is not None else None
+    om = _el(omega)
+    _check(lib().zkgpu_ntt_dev(dev, _ptr(t), log_n, om.ctypes.data, cc.ctypes.data if cc is not None else None,
+                               ps.ctypes.data if ps is not None else None, _stream_ptr(stream)), "ntt_dev")
+    del c
+
+
+def lagrange_to_extended_dev(values, ext, log_n: int, log_ext: int, omega_inv, divisor, g, omega_ext, stream=None):
+    dev = values.device.index
+    wi, d, gg, we = _el(omega_inv), _el(divisor), _el(g), _el(omega_ext)
+    _check(lib().zkgpu_lagrange_to_extended_dev(dev, _ptr(values), log_n, _ptr(ext), log_ext, wi.ctypes.data,
+                                                d.ctypes.data, gg.ctypes.data, we.ctypes.data, _stream_ptr(stream)),
+           "lagrange_to_extended_dev")
+
+
+def msm_dev(scalars, bases, out, stream=None):
+    dev = scalars.device.index
+    _check(lib().zkgpu_msm_dev(dev, _ptr(scalars), _ptr(bases), scalars.shape[0], _ptr(out), _stream_ptr(stream)),
+           "msm_dev")

@@ -1,0 +1,347 @@
+// field.cuh — BN254 Fr / Fq arithmetic for sm_100a on 8 x 32-bit limbs.
+//
+// Elements are 256-bit little-endian integers in Montgomery form with
+// R = 2^256 — bit-identical to the reference's BigNum (cuda/bn256.h:10-13,
+// 4 x u64 LE) and to halo2curves' Fr / Fq repr, so device buffers are the
+// host buffers reinterpreted.  The moduli (cuda/bn256.h:37, :54) are both
+// < 2^254, so 4p < R, which allows "lazy" forms:
+//   mul_lazy : a, b < 2p  ->  a*b*R^-1 mod p  in [0, 2p)   (no final subtract)
+//   add_lazy : a, b < 2p  ->  a + b           in [0, 2p)
+//   sub_lazy : a, b < 2p  ->  a - b           in [0, 2p)
+// and canonical forms (inputs < p, outputs < p) used where values are
+// compared.  Every carry chain lives inside ONE asm statement: the carry
+// flag is never assumed to survive between statements (the reference's
+// gpu_math.h:31-77 macros rely on that; this file does not).
+//
+// Montgomery multiplication is CIOS over 32-bit words; each iteration adds
+// a*b_i (lo then hi partial products, two madc chains), computes
+// m = T0 * (-p^-1 mod 2^32) and adds m*p the same way, then drops T0.
+// Cost: 8 x (33 IMAD + 2 IADD) per product, all on the integer pipes.
+#pragma once
+#include <cstdint>
+
+namespace zk {
+
+struct fe {
+  uint32_t w[8];
+};
+
+// ---- moduli (cuda/bn256.h:37-56) ----------------------------------------
+struct FrP {
+  static constexpr uint32_t P0 = 0xf0000001u, P1 = 0x43e1f593u, P2 = 0x79b97091u, P3 = 0x2833e848u,
+                            P4 = 0x8181585du, P5 = 0xb85045b6u, P6 = 0xe131a029u, P7 = 0x30644e72u;
+  static constexpr uint32_t INV = 0xefffffffu;  // -p^-1 mod 2^32
+  // R mod p (Montgomery one)
+  static constexpr uint32_t O0 = 0x4ffffffbu, O1 = 0xac96341cu, O2 = 0x9f60cd29u, O3 = 0x36fc7695u,
+                            O4 = 0x7879462eu, O5 = 0x666ea36fu, O6 = 0x9a07df2fu, O7 = 0x0e0a77c1u;
+};
+struct FqP {
+  static constexpr uint32_t P0 = 0xd87cfd47u, P1 = 0x3c208c16u, P2 = 0x6871ca8du, P3 = 0x97816a91u,
+                            P4 = 0x8181585du, P5 = 0xb85045b6u, P6 = 0xe131a029u, P7 = 0x30644e72u;
+  static constexpr uint32_t INV = 0xe4866389u;
+  static constexpr uint32_t O0 = 0xc58f0d9du, O1 = 0xd35d438du, O2 = 0xf5c70b3du, O3 = 0x0a78eb28u,
+                            O4 = 0x7879462cu, O5 = 0x666ea36fu, O6 = 0x9a07df2fu, O7 = 0x0e0a77c1u;
+};
+
+#define ZK_P_OPS(P) "n"(P::INV), "n"(P::P0), "n"(P::P1), "n"(P::P2), "n"(P::P3), "n"(P::P4), "n"(P::P5), "n"(P::P6), "n"(P::P7)
+
+// One CIOS iteration: T += a * b ; m = T0*inv ; T += m*p  (T is 9 words).
+// Operands: %0-%8 T, %9-%16 a, %17 b, %18 inv, %19-%26 p.
+#define ZK_CIOS_BODY                               \
+  "{\n\t.reg .u32 m;\n\t"                          \
+  "mad.lo.cc.u32  %0, %9, %17, %0;\n\t"            \
+  "madc.lo.cc.u32 %1, %10, %17, %1;\n\t"           \
+  "madc.lo.cc.u32 %2, %11, %17, %2;\n\t"           \
+  "madc.lo.cc.u32 %3, %12, %17, %3;\n\t"           \
+  "madc.lo.cc.u32 %4, %13, %17, %4;\n\t"           \
+  "madc.lo.cc.u32 %5, %14, %17, %5;\n\t"           \
+  "madc.lo.cc.u32 %6, %15, %17, %6;\n\t"           \
+  "madc.lo.cc.u32 %7, %16, %17, %7;\n\t"           \
+  "addc.u32       %8, %8, 0;\n\t"                  \
+  "mad.hi.cc.u32  %1, %9, %17, %1;\n\t"            \
+  "madc.hi.cc.u32 %2, %10, %17, %2;\n\t"           \
+  "madc.hi.cc.u32 %3, %11, %17, %3;\n\t"           \
+  "madc.hi.cc.u32 %4, %12, %17, %4;\n\t"           \
+  "madc.hi.cc.u32 %5, %13, %17, %5;\n\t"           \
+  "madc.hi.cc.u32 %6, %14, %17, %6;\n\t"           \
+  "madc.hi.cc.u32 %7, %15, %17, %7;\n\t"           \
+  "madc.hi.u32    %8, %16, %17, %8;\n\t"           \
+  "mul.lo.u32     m, %0, %18;\n\t"                 \
+  "mad.lo.cc.u32  %0, m, %19, %0;\n\t"             \
+  "madc.lo.cc.u32 %1, m, %20, %1;\n\t"             \
+  "madc.lo.cc.u32 %2, m, %21, %2;\n\t"             \
+  "madc.lo.cc.u32 %3, m, %22, %3;\n\t"             \
+  "madc.lo.cc.u32 %4, m, %23, %4;\n\t"             \
+  "madc.lo.cc.u32 %5, m, %24, %5;\n\t"             \
+  "madc.lo.cc.u32 %6, m, %25, %6;\n\t"             \
+  "madc.lo.cc.u32 %7, m, %26, %7;\n\t"             \
+  "addc.u32       %8, %8, 0;\n\t"                  \
+  "mad.hi.cc.u32  %1, m, %19, %1;\n\t"             \
+  "madc.hi.cc.u32 %2, m, %20, %2;\n\t"             \
+  "madc.hi.cc.u32 %3, m, %21, %3;\n\t"             \
+  "madc.hi.cc.u32 %4, m, %22, %4;\n\t"             \
+  "madc.hi.cc.u32 %5, m, %23, %5;\n\t"             \
+  "madc.hi.cc.u32 %6, m, %24, %6;\n\t"             \
+  "madc.hi.cc.u32 %7, m, %25, %7;\n\t"             \
+  "madc.hi.u32    %8, m, %26, %8;\n\t"             \
+  "}"
+
+// First iteration: T = a * b0 (T starts at zero), then the reduction step.
+#define ZK_CIOS_FIRST                              \
+  "{\n\t.reg .u32 m;\n\t"                          \
+  "mul.lo.u32     %0, %9, %17;\n\t"                \
+  "mul.lo.u32     %1, %10, %17;\n\t"               \
+  "mul.lo.u32     %2, %11, %17;\n\t"               \
+  "mul.lo.u32     %3, %12, %17;\n\t"               \
+  "mul.lo.u32     %4, %13, %17;\n\t"               \
+  "mul.lo.u32     %5, %14, %17;\n\t"               \
+  "mul.lo.u32     %6, %15, %17;\n\t"               \
+  "mul.lo.u32     %7, %16, %17;\n\t"               \
+  "mad.hi.cc.u32  %1, %9, %17, %1;\n\t"            \
+  "madc.hi.cc.u32 %2, %10, %17, %2;\n\t"           \
+  "madc.hi.cc.u32 %3, %11, %17, %3;\n\t"           \
+  "madc.hi.cc.u32 %4, %12, %17, %4;\n\t"           \
+  "madc.hi.cc.u32 %5, %13, %17, %5;\n\t"           \
+  "madc.hi.cc.u32 %6, %14, %17, %6;\n\t"           \
+  "madc.hi.cc.u32 %7, %15, %17, %7;\n\t"           \
+  "madc.hi.u32    %8, %16, %17, 0;\n\t"            \
+  "mul.lo.u32     m, %0, %18;\n\t"                 \
+  "mad.lo.cc.u32  %0, m, %19, %0;\n\t"             \
+  "madc.lo.cc.u32 %1, m, %20, %1;\n\t"             \
+  "madc.lo.cc.u32 %2, m, %21, %2;\n\t"             \
+  "madc.lo.cc.u32 %3, m, %22, %3;\n\t"             \
+  "madc.lo.cc.u32 %4, m, %23, %4;\n\t"             \
+  "madc.lo.cc.u32 %5, m, %24, %5;\n\t"             \
+  "madc.lo.cc.u32 %6, m, %25, %6;\n\t"             \
+  "madc.lo.cc.u32 %7, m, %26, %7;\n\t"             \
+  "addc.u32       %8, %8, 0;\n\t"                  \
+  "mad.hi.cc.u32  %1, m, %19, %1;\n\t"             \
+  "madc.hi.cc.u32 %2, m, %20, %2;\n\t"             \
+  "madc.hi.cc.u32 %3, m, %21, %3;\n\t"             \
+  "madc.hi.cc.u32 %4, m, %22, %4;\n\t"             \
+  "madc.hi.cc.u32 %5, m, %23, %5;\n\t"             \
+  "madc.hi.cc.u32 %6, m, %24, %6;\n\t"             \
+  "madc.hi.cc.u32 %7, m, %25, %7;\n\t"             \
+  "madc.hi.u32    %8, m, %26, %8;\n\t"             \
+  "}"
+
+#define ZK_T_OPS(T) "+r"(T[0]), "+r"(T[1]), "+r"(T[2]), "+r"(T[3]), "+r"(T[4]), "+r"(T[5]), "+r"(T[6]), "+r"(T[7]), "+r"(T[8])
+#define ZK_A_OPS(a) "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7])
+
+// r = a*b*R^-1 mod p, for a, b < 2p: result < 2p.
+template <class P>
+__device__ __forceinline__ void mul_lazy(uint32_t r[8], const uint32_t a[8], const uint32_t b[8]) {
+  uint32_t T[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  asm(ZK_CIOS_FIRST : ZK_T_OPS(T) : ZK_A_OPS(a), "r"(b[0]), ZK_P_OPS(P));
+#pragma unroll
+  for (int i = 1; i < 8; i++) {
+    // shift: drop T0 (zero), T8 becomes the new top, new T8 = 0
+#pragma unroll
+    for (int j = 0; j < 8; j++) T[j] = T[j + 1];
+    T[8] = 0;
+    asm(ZK_CIOS_BODY : ZK_T_OPS(T) : ZK_A_OPS(a), "r"(b[i]), ZK_P_OPS(P));
+  }
+#pragma unroll
+  for (int j = 0; j < 8; j++) r[j] = T[j + 1];
+}
+
+// r = a + b - 2p if that does not borrow, else a + b.  Inputs < 2p.
+template <class P>
+__device__ __forceinline__ void add_lazy(uint32_t r[8], const uint32_t a[8], const uint32_t b[8]) {
+  uint32_t s[8], t[8], borrow;
+  asm("add.cc.u32  %0, %8, %16;\n\t"
+      "addc.cc.u32 %1, %9, %17;\n\t"
+      "addc.cc.u32 %2, %10, %18;\n\t"
+      "addc.cc.u32 %3, %11, %19;\n\t"
+      "addc.cc.u32 %4, %12, %20;\n\t"
+      "addc.cc.u32 %5, %13, %21;\n\t"
+      "addc.cc.u32 %6, %14, %22;\n\t"
+      "addc.u32    %7, %15, %23;"
+      : "=r"(s[0]), "=r"(s[1]), "=r"(s[2]), "=r"(s[3]), "=r"(s[4]), "=r"(s[5]), "=r"(s[6]), "=r"(s[7])
+      : ZK_A_OPS(a), ZK_A_OPS(b));
+  // t = s - 2p
+  asm("sub.cc.u32  %0, %9, %17;\n\t"
+      "subc.cc.u32 %1, %10, %18;\n\t"
+      "subc.cc.u32 %2, %11, %19;\n\t"
+      "subc.cc.u32 %3, %12, %20;\n\t"
+      "subc.cc.u32 %4, %13, %21;\n\t"
+      "subc.cc.u32 %5, %14, %22;\n\t"
+      "subc.cc.u32 %6, %15, %23;\n\t"
+      "subc.cc.u32 %7, %16, %24;\n\t"
+      "subc.u32    %8, 0, 0;"
+      : "=r"(t[0]), "=r"(t[1]), "=r"(t[2]), "=r"(t[3]), "=r"(t[4]), "=r"(t[5]), "=r"(t[6]), "=r"(t[7]), "=r"(borrow)
+      : ZK_A_OPS(s), "n"((uint32_t)(P::P0 << 1)), "n"((P::P1 << 1) | (P::P0 >> 31)), "n"((P::P2 << 1) | (P::P1 >> 31)),
+        "n"((P::P3 << 1) | (P::P2 >> 31)), "n"((P::P4 << 1) | (P::P3 >> 31)), "n"((P::P5 << 1) | (P::P4 >> 31)),
+        "n"((P::P6 << 1) | (P::P5 >> 31)), "n"((P::P7 << 1) | (P::P6 >> 31)));
+#pragma unroll
+  for (int j = 0; j < 8; j++) r[j] = borrow ? s[j] : t[j];
+}
+
+// r = a - b, plus 2p if that borrowed.  Inputs < 2p.
+template <class P>
+__device__ __forceinline__ void sub_lazy(uint32_t r[8], const uint32_t a[8], const uint32_t b[8]) {
+  uint32_t d[8], borrow;
+  asm("sub.cc.u32  %0, %9, %17;\n\t"
+      "subc.cc.u32 %1, %10, %18;\n\t"
+      "subc.cc.u32 %2, %11, %19;\n\t"
+      "subc.cc.u32 %3, %12, %20;\n\t"
+      "subc.cc.u32 %4, %13, %21;\n\t"
+      "subc.cc.u32 %5, %14, %22;\n\t"
+      "subc.cc.u32 %6, %15, %23;\n\t"
+      "subc.cc.u32 %7, %16, %24;\n\t"
+      "subc.u32    %8, 0, 0;"
+      : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]), "=r"(borrow)
+      : ZK_A_OPS(a), ZK_A_OPS(b));
+  // conditional + 2p (mask form keeps it branch-free)
+  const uint32_t mk = borrow;  // 0 or 0xffffffff
+  asm("add.cc.u32  %0, %0, %8;\n\t"
+      "addc.cc.u32 %1, %1, %9;\n\t"
+      "addc.cc.u32 %2, %2, %10;\n\t"
+      "addc.cc.u32 %3, %3, %11;\n\t"
+      "addc.cc.u32 %4, %4, %12;\n\t"
+      "addc.cc.u32 %5, %5, %13;\n\t"
+      "addc.cc.u32 %6, %6, %14;\n\t"
+      "addc.u32    %7, %7, %15;"
+      : "+r"(d[0]), "+r"(d[1]), "+r"(d[2]), "+r"(d[3]), "+r"(d[4]), "+r"(d[5]), "+r"(d[6]), "+r"(d[7])
+      : "r"(mk & (uint32_t)(P::P0 << 1)), "r"(mk & ((P::P1 << 1) | (P::P0 >> 31))), "r"(mk & ((P::P2 << 1) | (P::P1 >> 31))),
+        "r"(mk & ((P::P3 << 1) | (P::P2 >> 31))), "r"(mk & ((P::P4 << 1) | (P::P3 >> 31))),
+        "r"(mk & ((P::P5 << 1) | (P::P4 >> 31))), "r"(mk & ((P::P6 << 1) | (P::P5 >> 31))),
+        "r"(mk & ((P::P7 << 1) | (P::P6 >> 31))));
+#pragma unroll
+  for (int j = 0; j < 8; j++) r[j] = d[j];
+}
+
+// Reduce a value < 2p to canonical [0, p).
+template <class P>
+__device__ __forceinline__ void reduce_once(uint32_t r[8], const uint32_t a[8]) {
+  uint32_t t[8], borrow;
+  asm("sub.cc.u32  %0, %9, %17;\n\t"
+      "subc.cc.u32 %1, %10, %18;\n\t"
+      "subc.cc.u32 %2, %11, %19;\n\t"
+      "subc.cc.u32 %3, %12, %20;\n\t"
+      "subc.cc.u32 %4, %13, %21;\n\t"
+      "subc.cc.u32 %5, %14, %22;\n\t"
+      "subc.cc.u32 %6, %15, %23;\n\t"
+      "subc.cc.u32 %7, %16, %24;\n\t"
+      "subc.u32    %8, 0, 0;"
+      : "=r"(t[0]), "=r"(t[1]), "=r"(t[2]), "=r"(t[3]), "=r"(t[4]), "=r"(t[5]), "=r"(t[6]), "=r"(t[7]), "=r"(borrow)
+      : ZK_A_OPS(a), "n"(P::P0), "n"(P::P1), "n"(P::P2), "n"(P::P3), "n"(P::P4), "n"(P::P5), "n"(P::P6), "n"(P::P7));
+#pragma unroll
+  for (int j = 0; j < 8; j++) r[j] = borrow ? a[j] : t[j];
+}
+
+// ---- canonical forms (inputs < p, outputs < p) ---------------------------
+template <class P>
+__device__ __forceinline__ void mul(uint32_t r[8], const uint32_t a[8], const uint32_t b[8]) {
+  uint32_t t[8];
+  mul_lazy<P>(t, a, b);
+  reduce_once<P>(r, t);
+}
+template <class P>
+__device__ __forceinline__ void sqr(uint32_t r[8], const uint32_t a[8]) {
+  mul<P>(r, a, a);
+}
+template <class P>
+__device__ __forceinline__ void add(uint32_t r[8], const uint32_t a[8], const uint32_t b[8]) {
+  uint32_t s[8];
+  asm("add.cc.u32  %0, %8, %16;\n\t"
+      "addc.cc.u32 %1, %9, %17;\n\t"
+      "addc.cc.u32 %2, %10, %18;\n\t"
+      "addc.cc.u32 %3, %11, %19;\n\t"
+      "addc.cc.u32 %4, %12, %20;\n\t"
+      "addc.cc.u32 %5, %13, %21;\n\t"
+      "addc.cc.u32 %6, %14, %22;\n\t"
+      "addc.u32    %7, %15, %23;"
+      : "=r"(s[0]), "=r"(s[1]), "=r"(s[2]), "=r"(s[3]), "=r"(s[4]), "=r"(s[5]), "=r"(s[6]), "=r"(s[7])
+      : ZK_A_OPS(a), ZK_A_OPS(b));
+  reduce_once<P>(r, s);
+}
+template <class P>
+__device__ __forceinline__ void sub(uint32_t r[8], const uint32_t a[8], const uint32_t b[8]) {
+  uint32_t d[8], borrow;
+  asm("sub.cc.u32  %0, %9, %17;\n\t"
+      "subc.cc.u32 %1, %10, %18;\n\t"
+      "subc.cc.u32 %2, %11, %19;\n\t"
+      "subc.cc.u32 %3, %12, %20;\n\t"
+      "subc.cc.u32 %4, %13, %21;\n\t"
+      "subc.cc.u32 %5, %14, %22;\n\t"
+      "subc.cc.u32 %6, %15, %23;\n\t"
+      "subc.cc.u32 %7, %16, %24;\n\t"
+      "subc.u32    %8, 0, 0;"
+      : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]), "=r"(borrow)
+      : ZK_A_OPS(a), ZK_A_OPS(b));
+  const uint32_t mk = borrow;
+  asm("add.cc.u32  %0, %0, %8;\n\t"
+      "addc.cc.u32 %1, %1, %9;\n\t"
+      "addc.cc.u32 %2, %2, %10;\n\t"
+      "addc.cc.u32 %3, %3, %11;\n\t"
+      "addc.cc.u32 %4, %4, %12;\n\t"
+      "addc.cc.u32 %5, %5, %13;\n\t"
+      "addc.cc.u32 %6, %6, %14;\n\t"
+      "addc.u32    %7, %7, %15;"
+      : "+r"(d[0]), "+r"(d[1]), "+r"(d[2]), "+r"(d[3]), "+r"(d[4]), "+r"(d[5]), "+r"(d[6]), "+r"(d[7])
+      : "r"(mk & P::P0), "r"(mk & P::P1), "r"(mk & P::P2), "r"(mk & P::P3), "r"(mk & P::P4), "r"(mk & P::P5),
+        "r"(mk & P::P6), "r"(mk & P::P7));
+#pragma unroll
+  for (int j = 0; j < 8; j++) r[j] = d[j];
+}
+template <class P>
+__device__ __forceinline__ void dbl(uint32_t r[8], const uint32_t a[8]) {
+  add<P>(r, a, a);
+}
+
+__device__ __forceinline__ bool is_zero(const uint32_t a[8]) {
+  return (a[0] | a[1] | a[2] | a[3] | a[4] | a[5] | a[6] | a[7]) == 0;
+}
+__device__ __forceinline__ bool eq(const uint32_t a[8], const uint32_t b[8]) {
+  return ((a[0] ^ b[0]) | (a[1] ^ b[1]) | (a[2] ^ b[2]) | (a[3] ^ b[3]) | (a[4] ^ b[4]) | (a[5] ^ b[5]) |
+          (a[6] ^ b[6]) | (a[7] ^ b[7])) == 0;
+}
+template <class P>
+__device__ __forceinline__ void set_one(uint32_t r[8]) {
+  r[0] = P::O0; r[1] = P::O1; r[2] = P::O2; r[3] = P::O3;
+  r[4] = P::O4; r[5] = P::O5; r[6] = P::O6; r[7] = P::O7;
+}
+__device__ __forceinline__ void set_zero(uint32_t r[8]) {
+#pragma unroll
+  for (int j = 0; j < 8; j++) r[j] = 0;
+}
+__device__ __forceinline__ void cpy(uint32_t r[8], const uint32_t a[8]) {
+#pragma unroll
+  for (int j = 0; j < 8; j++) r[j] = a[j];
+}
+
+// a^e for a small exponent (canonical inputs), square-and-multiply
+template <class P>
+__device__ __forceinline__ void pow_u64(uint32_t r[8], const uint32_t a[8], uint64_t e) {
+  uint32_t acc[8], base[8];
+  set_one<P>(acc);
+  cpy(base, a);
+  while (e) {
+    if (e & 1) mul<P>(acc, acc, base);
+    e >>= 1;
+    if (e) sqr<P>(base, base);
+  }
+  cpy(r, acc);
+}
+
+// ---- global memory element access (32 B = one sector, two 16 B vectors) --
+__device__ __forceinline__ void ld_fe(uint32_t r[8], const fe* p) {
+  const uint4* q = reinterpret_cast<const uint4*>(p);
+  uint4 x = q[0], y = q[1];
+  r[0] = x.x; r[1] = x.y; r[2] = x.z; r[3] = x.w;
+  r[4] = y.x; r[5] = y.y; r[6] = y.z; r[7] = y.w;
+}
+__device__ __forceinline__ void ld_fe_nc(uint32_t r[8], const fe* p) {
+  const uint4* q = reinterpret_cast<const uint4*>(p);
+  uint4 x = __ldg(q), y = __ldg(q + 1);
+  r[0] = x.x; r[1] = x.y; r[2] = x.z; r[3] = x.w;
+  r[4] = y.x; r[5] = y.y; r[6] = y.z; r[7] = y.w;
+}
+__device__ __forceinline__ void st_fe(fe* p, const uint32_t r[8]) {
+  uint4* q = reinterpret_cast<uint4*>(p);
+  q[0] = make_uint4(r[0], r[1], r[2], r[3]);
+  q[1] = make_uint4(r[4], r[5], r[6], r[7]);
+}
+
+}  // namespace zk

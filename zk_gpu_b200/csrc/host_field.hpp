@@ -1,0 +1,128 @@
+// host_field.hpp — host-side Fr arithmetic for the library's own bookkeeping
+// (root-of-unity checks, per-pass roots, LDE constants).  4 x u64 little
+// endian Montgomery limbs, the layout of cuda/bn256.h:10-13.  Not on the hot
+// path: a few hundred products per call at most.
+#pragma once
+#include <cstdint>
+#include <cstring>
+
+namespace zk {
+namespace host {
+
+struct Fr {
+  uint64_t v[4];
+};
+
+static constexpr uint64_t R_P[4] = {0x43e1f593f0000001ULL, 0x2833e84879b97091ULL, 0xb85045b68181585dULL,
+                                    0x30644e72e131a029ULL};
+static constexpr uint64_t R_INV = 0xc2e1f593efffffffULL;
+static constexpr uint64_t R_ONE[4] = {0xac96341c4ffffffbULL, 0x36fc76959f60cd29ULL, 0x666ea36f7879462eULL,
+                                      0x0e0a77c19a07df2fULL};
+static constexpr uint64_t R_R2[4] = {0x1bb8e645ae216da7ULL, 0x53fe3ab1e35c59e3ULL, 0x8c49833d53bb8085ULL,
+                                     0x0216d0b17f4e44a5ULL};
+
+inline bool geq(const uint64_t a[4], const uint64_t b[4]) {
+  for (int i = 3; i >= 0; i--) {
+    if (a[i] != b[i]) return a[i] > b[i];
+  }
+  return true;
+}
+inline void sub_p(uint64_t a[4]) {
+  unsigned __int128 br = 0;
+  for (int i = 0; i < 4; i++) {
+    unsigned __int128 d = (unsigned __int128)a[i] - R_P[i] - (uint64_t)br;
+    a[i] = (uint64_t)d;
+    br = (d >> 64) & 1;
+  }
+}
+inline bool is_canonical(const Fr& a) { return !geq(a.v, R_P); }
+
+inline Fr mul(const Fr& a, const Fr& b) {
+  uint64_t t[6] = {0, 0, 0, 0, 0, 0};
+  for (int i = 0; i < 4; i++) {
+    uint64_t c = 0;
+    for (int j = 0; j < 4; j++) {
+      unsigned __int128 s = (unsigned __int128)a.v[j] * b.v[i] + t[j] + c;
+      t[j] = (uint64_t)s;
+      c = (uint64_t)(s >> 64);
+    }
+    unsigned __int128 s = (unsigned __int128)t[4] + c;
+    t[4] = (uint64_t)s;
+    t[5] = (uint64_t)(s >> 64);
+    uint64_t m = t[0] * R_INV;
+    s = (unsigned __int128)m * R_P[0] + t[0];
+    c = (uint64_t)(s >> 64);
+    for (int j = 1; j < 4; j++) {
+      s = (unsigned __int128)m * R_P[j] + t[j] + c;
+      t[j - 1] = (uint64_t)s;
+      c = (uint64_t)(s >> 64);
+    }
+    s = (unsigned __int128)t[4] + c;
+    t[3] = (uint64_t)s;
+    t[4] = t[5] + (uint64_t)(s >> 64);
+  }
+  Fr r;
+  std::memcpy(r.v, t, sizeof(r.v));
+  if (t[4] || geq(r.v, R_P)) sub_p(r.v);
+  return r;
+}
+inline Fr one() {
+  Fr r;
+  std::memcpy(r.v, R_ONE, sizeof(r.v));
+  return r;
+}
+inline Fr zero() {
+  Fr r{{0, 0, 0, 0}};
+  return r;
+}
+inline Fr from_u64(uint64_t x) {
+  Fr c{{x, 0, 0, 0}}, r2;
+  std::memcpy(r2.v, R_R2, sizeof(r2.v));
+  return mul(c, r2);
+}
+inline bool eq(const Fr& a, const Fr& b) { return std::memcmp(a.v, b.v, sizeof(a.v)) == 0; }
+inline Fr neg(const Fr& a) {
+  if (!(a.v[0] | a.v[1] | a.v[2] | a.v[3])) return a;
+  Fr r;
+  unsigned __int128 br = 0;
+  for (int i = 0; i < 4; i++) {
+    unsigned __int128 d = (unsigned __int128)R_P[i] - a.v[i] - (uint64_t)br;
+    r.v[i] = (uint64_t)d;
+    br = (d >> 64) & 1;
+  }
+  return r;
+}
+inline Fr pow_u64(Fr a, uint64_t e) {
+  Fr r = one();
+  while (e) {
+    if (e & 1) r = mul(r, a);
+    e >>= 1;
+    if (e) a = mul(a, a);
+  }
+  return r;
+}
+inline Fr pow_2k(Fr a, unsigned k) {  // a^(2^k)
+  for (unsigned i = 0; i < k; i++) a = mul(a, a);
+  return a;
+}
+inline Fr inv(const Fr& a) {  // Fermat: a^(r-2)
+  uint64_t e[4];
+  std::memcpy(e, R_P, sizeof(e));
+  e[0] -= 2;
+  Fr r = one();
+  for (int i = 3; i >= 0; i--)
+    for (int b = 63; b >= 0; b--) {
+      r = mul(r, r);
+      if ((e[i] >> b) & 1) r = mul(r, a);
+    }
+  return r;
+}
+// true iff w has multiplicative order exactly 2^log_n (w^(n/2) == -1)
+inline bool is_primitive_root(const Fr& w, unsigned log_n) {
+  if (log_n == 0) return eq(w, one());
+  Fr h = pow_2k(w, log_n - 1);
+  return eq(h, neg(one()));
+}
+
+}  // namespace host
+}  // namespace zk

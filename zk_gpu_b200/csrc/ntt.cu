@@ -1,0 +1,542 @@
+// ntt.cu — Fr NTT pass kernels and host orchestration (see ntt.cuh).
+//
+// Per pass, one CTA owns G columns of one outer block (or, in the last pass,
+// G groups whose outputs are adjacent).  Each thread holds 8 elements of one
+// column and runs the m-point DIF DFT as "rounds": a round covers three
+// index bits [lo, lo+3) that the thread holds in registers and performs the
+// radix-2 stages whose butterfly bit falls in that range.  Between rounds the
+// column is exchanged through shared memory, stored as 8 u32 planes with the
+// XOR swizzle  addr = e ^ ((e >> 3) & 31),  which keeps every round's
+// 32-lane access pattern on 32 distinct banks for all b in [3, 12].
+// Twiddles of the last round are the 8th roots of unity (compile-time
+// indices, broadcast reads); the w == 1 butterflies skip the product.
+// Values stay in [0, 2p) between stages (lazy reduction, 4p < 2^256) and
+// are made canonical on the final store.
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
+#include "ntt.cuh"
+#include "prof.cuh"
+
+namespace zk {
+
+using P_r = FrP;
+
+NttPlan make_ntt_plan(int log_n) {
+  NttPlan p;
+  p.log_n = log_n;
+  if (log_n <= 2) {  // direct DFT kernel
+    p.npass = 0;
+    return p;
+  }
+  if (log_n <= 12) {
+    p.npass = 1;
+    p.bits[0] = log_n;
+    return p;
+  }
+  int np = (log_n + 8) / 9;  // passes of at most 9 bits
+  if (np < 2) np = 2;
+  p.npass = np;
+  int base = log_n / np, extra = log_n % np;
+  for (int t = 0; t < np; t++) p.bits[t] = base + (t < extra ? 1 : 0);
+  return p;
+}
+
+// ---------------------------------------------------------------------------
+// device helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t swz(uint32_t e) { return e ^ ((e >> 3) & 31u); }
+
+template <int LO>
+__device__ __forceinline__ uint32_t ins3(uint32_t q, uint32_t r) {
+  return (q & ((1u << LO) - 1u)) | (r << LO) | ((q >> LO) << (LO + 3));
+}
+
+__device__ __forceinline__ void ld_smem_fe(uint32_t r[8], const uint32_t* plane0, uint32_t plane_stride, uint32_t a) {
+#pragma unroll
+  for (int k = 0; k < 8; k++) r[k] = plane0[k * plane_stride + a];
+}
+__device__ __forceinline__ void st_smem_fe(uint32_t* plane0, uint32_t plane_stride, uint32_t a, const uint32_t r[8]) {
+#pragma unroll
+  for (int k = 0; k < 8; k++) plane0[k * plane_stride + a] = r[k];
+}
+
+// One round: registers hold i(r) = ins3<LO>(q, r); perform the DIF stages
+// with butterfly bits HI-1 .. LO.  tws: inner roots w_m^e (e < m/2), 8 planes.
+template <int B, int LO, int HI>
+__device__ __forceinline__ void ntt_round(uint32_t x[8][8], uint32_t q, const uint32_t* tws) {
+  constexpr uint32_t HALF = 1u << (B - 1);
+#pragma unroll
+  for (int b = HI - 1; b >= LO; b--) {
+    const int rb = b - LO;
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      if (r & (1 << rb)) continue;
+      const int r2 = r | (1 << rb);
+      uint32_t t[8];
+      sub_lazy<P_r>(t, x[r], x[r2]);
+      add_lazy<P_r>(x[r], x[r], x[r2]);
+      if constexpr (LO == 0) {
+        // exponent is a compile-time constant: (r mod 2^b) << (B-1-b)
+        const uint32_t e = (uint32_t)(r & ((1 << b) - 1)) << (B - 1 - b);
+        if (e == 0) {
+#pragma unroll
+          for (int k = 0; k < 8; k++) x[r2][k] = t[k];
+        } else {
+          uint32_t w[8];
+          ld_smem_fe(w, tws, HALF, e);
+          mul_lazy<P_r>(x[r2], t, w);
+        }
+      } else {
+        const uint32_t e = ((q & ((1u << LO) - 1u)) | ((uint32_t)(r & ((1 << rb) - 1)) << LO)) << (B - 1 - b);
+        uint32_t w[8];
+        ld_smem_fe(w, tws, HALF, e);
+        mul_lazy<P_r>(x[r2], t, w);
+      }
+    }
+  }
+}
+
+template <int B, int LO_CUR, int LO_NEXT>
+__device__ __forceinline__ void ntt_exchange(uint32_t x[8][8], uint32_t q, uint32_t gbase, uint32_t* sm,
+                                             uint32_t plane_stride) {
+#pragma unroll
+  for (int r = 0; r < 8; r++) st_smem_fe(sm, plane_stride, swz(gbase + ins3<LO_CUR>(q, r)), x[r]);
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < 8; r++) ld_smem_fe(x[r], sm, plane_stride, swz(gbase + ins3<LO_NEXT>(q, r)));
+  __syncthreads();
+}
+
+template <int B, int HI>
+__device__ __forceinline__ void ntt_rounds(uint32_t x[8][8], uint32_t q, uint32_t gbase, uint32_t* sm,
+                                           uint32_t plane_stride, const uint32_t* tws) {
+  constexpr int LO = HI - 3 > 0 ? HI - 3 : 0;
+  ntt_round<B, LO, HI>(x, q, tws);
+  if constexpr (LO > 0) {
+    constexpr int LO_N = LO - 3 > 0 ? LO - 3 : 0;
+    ntt_exchange<B, LO, LO_N>(x, q, gbase, sm, plane_stride);
+    ntt_rounds<B, LO>(x, q, gbase, sm, plane_stride, tws);
+  }
+}
+
+struct PassParams {
+  const fe* in;
+  fe* out;
+  const fe* inner;   // w_m^e, e < m/2
+  const fe* twist;   // [k * J + j], non-final passes
+  const fe* pre_lo;  // coset powers (first pass), or null
+  const fe* pre_hi;
+  uint32_t pre_shift;
+  uint32_t log_J;
+  uint32_t log_O;
+  uint32_t log_m1;
+  uint32_t nprev;
+  uint32_t prev_bits[NTT_MAX_PASS];
+  uint32_t G;
+  uint32_t is_final;
+  uint32_t has_post;
+  fe post;
+};
+
+template <int B>
+__global__ void __launch_bounds__(B >= 12 ? 512 : 256, B >= 12 ? 1 : 2) ntt_pass_kernel(const PassParams p) {
+  constexpr uint32_t M = 1u << B;
+  constexpr uint32_t T = M / 8;  // threads per column
+  extern __shared__ uint32_t smem[];
+  const uint32_t G = p.G;
+  const uint32_t plane_stride = G * M;
+  uint32_t* tws = smem + 8 * plane_stride;
+
+  const uint32_t tid = threadIdx.x;
+  const uint32_t g = tid / T, q = tid % T;
+
+  for (uint32_t e = tid; e < M / 2; e += blockDim.x) {
+    uint32_t w[8];
+    ld_fe_nc(w, p.inner + e);
+    st_smem_fe(tws, M / 2, e, w);
+  }
+
+  const uint64_t J = 1ull << p.log_J;
+  uint64_t o, col = 0, base, stride;
+  if (!p.is_final) {
+    const uint64_t cols_per_o = J / G;
+    o = blockIdx.x / cols_per_o;
+    col = (blockIdx.x % cols_per_o) * G + g;
+    base = o * (uint64_t)M * J + col;
+    stride = J;
+  } else {
+    const uint64_t rest_count = (1ull << p.log_O) >> p.log_m1;
+    const uint64_t rest = blockIdx.x % rest_count;
+    const uint64_t k1 = (blockIdx.x / rest_count) * G + g;
+    o = k1 * rest_count + rest;
+    base = o * M;
+    stride = 1;
+  }
+
+  uint32_t x[8][8];
+#pragma unroll
+  for (int r = 0; r < 8; r++) ld_fe(x[r], p.in + base + (uint64_t)(q + T * r) * stride);
+
+  if (p.pre_lo) {
+    const uint64_t mask = (1ull << p.pre_shift) - 1;
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      const uint64_t xi = base + (uint64_t)(q + T * r) * stride;  // first pass: global input index
+      uint32_t a[8], b[8];
+      ld_fe_nc(a, p.pre_lo + (xi & mask));
+      ld_fe_nc(b, p.pre_hi + (xi >> p.pre_shift));
+      mul_lazy<P_r>(a, a, b);
+      mul_lazy<P_r>(x[r], x[r], a);
+    }
+  }
+  __syncthreads();
+
+  ntt_rounds<B, B>(x, q, g * M, smem, plane_stride, tws);
+
+  // element r now holds output k = bitrev_B(8q + r)
+  if (!p.is_final) {
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      const uint32_t k = __brev(8 * q + r) >> (32 - B);
+      uint32_t w[8];
+      ld_fe_nc(w, p.twist + (uint64_t)k * J + col);
+      mul_lazy<P_r>(x[r], x[r], w);
+      st_fe(p.out + o * (uint64_t)M * J + (uint64_t)k * J + col, x[r]);
+    }
+  } else {
+    // rev(o): o = k_1 * 2^(b_2+..) + ... + k_(p-1);  rev = k_1 + 2^b_1 k_2 + ...
+    uint64_t rev = 0, rem = o;
+    uint32_t low_bits = 0, total = 0;
+#pragma unroll
+    for (int t = 0; t < NTT_MAX_PASS; t++)
+      if (t < (int)p.nprev) total += p.prev_bits[t];
+    uint32_t above = total;
+#pragma unroll
+    for (int t = 0; t < NTT_MAX_PASS; t++) {
+      if (t < (int)p.nprev) {
+        above -= p.prev_bits[t];
+        const uint64_t digit = rem >> above;
+        rem &= (1ull << above) - 1;
+        rev |= digit << low_bits;
+        low_bits += p.prev_bits[t];
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      const uint32_t k = __brev(8 * q + r) >> (32 - B);
+      uint32_t v[8];
+      if (p.has_post) {
+        mul_lazy<P_r>(v, x[r], p.post.w);
+        reduce_once<P_r>(v, v);
+      } else {
+        reduce_once<P_r>(v, x[r]);
+      }
+      st_fe(p.out + rev + ((uint64_t)k << total), v);
+    }
+  }
+}
+
+// Tiny transforms (n <= 4): direct DFT, one thread per output.
+__global__ void ntt_tiny_kernel(fe* a, uint32_t log_n, fe w, const fe* pre_lo, const fe* pre_hi, uint32_t pre_shift,
+                                uint32_t has_post, fe post) {
+  const uint32_t n = 1u << log_n;
+  const uint32_t k = threadIdx.x;
+  uint32_t in[4][8];
+  for (uint32_t i = 0; i < n; i++) {
+    ld_fe(in[i], a + i);
+    if (pre_lo) {
+      uint32_t c0[8], c1[8];
+      ld_fe_nc(c0, pre_lo + (i & ((1u << pre_shift) - 1)));
+      ld_fe_nc(c1, pre_hi + (i >> pre_shift));
+      mul<P_r>(c0, c0, c1);
+      mul<P_r>(in[i], in[i], c0);
+    }
+  }
+  uint32_t acc[8];
+  if (k < n) {
+    uint32_t wk[8], wik[8];
+    pow_u64<P_r>(wk, w.w, k);
+    set_zero(acc);
+    set_one<P_r>(wik);
+    for (uint32_t i = 0; i < n; i++) {
+      uint32_t t[8];
+      mul<P_r>(t, in[i], wik);
+      add<P_r>(acc, acc, t);
+      mul<P_r>(wik, wik, wk);
+    }
+    if (has_post) mul<P_r>(acc, acc, post.w);
+  }
+  __syncthreads();
+  if (k < n) st_fe(a + k, acc);
+}
+
+// out[e] = base^(e) for e < count (per-thread square-and-multiply)
+__global__ void pow_seq_kernel(fe* out, fe base, uint64_t count, uint64_t step) {
+  const uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (e >= count) return;
+  uint32_t r[8];
+  pow_u64<P_r>(r, base.w, e * step);
+  st_fe(out + e, r);
+}
+
+// twist[k * J + j] = lo[(k j) & mask] * hi[(k j) >> shift]
+__global__ void twist_table_kernel(fe* out, const fe* lo, const fe* hi, uint32_t shift, uint32_t log_J, uint64_t total) {
+  const uint64_t idx = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (idx >= total) return;
+  const uint64_t k = idx >> log_J, j = idx & ((1ull << log_J) - 1);
+  const uint64_t e = k * j;
+  uint32_t a[8], b[8];
+  ld_fe_nc(a, lo + (e & ((1ull << shift) - 1)));
+  ld_fe_nc(b, hi + (e >> shift));
+  mul<P_r>(a, a, b);
+  st_fe(out + idx, a);
+}
+
+// dst[i * dst_stride] = src[i] * c^i (powc may be null: plain strided copy)
+__global__ void scale_copy_kernel(fe* dst, const fe* src, uint64_t n, uint64_t dst_stride, const fe* lo, const fe* hi,
+                                  uint32_t shift) {
+  const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t v[8];
+  ld_fe(v, src + i);
+  if (lo) {
+    uint32_t a[8], b[8];
+    ld_fe_nc(a, lo + (i & ((1ull << shift) - 1)));
+    ld_fe_nc(b, hi + (i >> shift));
+    mul_lazy<P_r>(a, a, b);
+    mul<P_r>(v, v, a);
+  }
+  st_fe(dst + i * dst_stride, v);
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+static fe to_fe(const host::Fr& a) {
+  fe r;
+  std::memcpy(r.w, a.v, 32);
+  return r;
+}
+
+static cudaError_t pow_two_level(fe** lo, fe** hi, uint32_t* shift, const host::Fr& base, int log_count,
+                                 cudaStream_t s, bool pooled) {
+  const uint32_t sh = (uint32_t)((log_count + 1) / 2);
+  const uint64_t nlo = 1ull << sh, nhi = 1ull << (log_count > (int)sh ? log_count - sh : 0);
+  cudaError_t e;
+  if (pooled) {
+    e = cudaMallocAsync((void**)lo, nlo * sizeof(fe), s);
+    if (e != cudaSuccess) return e;
+    e = cudaMallocAsync((void**)hi, nhi * sizeof(fe), s);
+    if (e != cudaSuccess) return e;
+  } else {
+    e = cudaMalloc((void**)lo, nlo * sizeof(fe));
+    if (e != cudaSuccess) return e;
+    e = cudaMalloc((void**)hi, nhi * sizeof(fe));
+    if (e != cudaSuccess) return e;
+  }
+  const host::Fr bstep = host::pow_2k(base, sh);
+  pow_seq_kernel<<<(unsigned)((nlo + 255) / 256), 256, 0, s>>>(*lo, to_fe(base), nlo, 1);
+  pow_seq_kernel<<<(unsigned)((nhi + 255) / 256), 256, 0, s>>>(*hi, to_fe(bstep), nhi, 1);
+  *shift = sh;
+  return cudaGetLastError();
+}
+
+cudaError_t pow_tables_make(PowTables* t, const host::Fr& c, int log_n, cudaStream_t s) {
+  return pow_two_level(&t->lo, &t->hi, &t->shift, c, log_n, s, true);
+}
+void pow_tables_free(PowTables* t, cudaStream_t s) {
+  if (t->lo) cudaFreeAsync(t->lo, s);
+  if (t->hi) cudaFreeAsync(t->hi, s);
+  t->lo = t->hi = nullptr;
+}
+
+namespace {
+struct Key {
+  int dev;
+  int log_n;
+  uint64_t w[4];
+  bool operator<(const Key& o) const {
+    return std::tie(dev, log_n, w[0], w[1], w[2], w[3]) < std::tie(o.dev, o.log_n, o.w[0], o.w[1], o.w[2], o.w[3]);
+  }
+};
+std::mutex g_mu;
+std::map<Key, std::unique_ptr<NttTables>> g_cache;
+}  // namespace
+
+static cudaError_t build_tables(NttTables* t, cudaStream_t s) {
+  const NttPlan& p = t->plan;
+  int done_bits = 0;
+  cudaError_t e = cudaSuccess;
+  for (int k = 0; k < p.npass; k++) {
+    const int b = p.bits[k];
+    const int log_J = p.log_n - done_bits - b;  // later passes' bits
+    // this pass works on the sub-problem of size m*J whose root is w^(n / (m J))
+    const host::Fr wMJ = host::pow_2k(t->omega, (unsigned)done_bits);
+    const host::Fr wm = host::pow_2k(wMJ, (unsigned)log_J);
+    const uint64_t half = b >= 1 ? (1ull << (b - 1)) : 1;
+    e = cudaMalloc((void**)&t->inner[k], half * sizeof(fe));
+    if (e != cudaSuccess) return e;
+    t->bytes += half * sizeof(fe);
+    pow_seq_kernel<<<(unsigned)((half + 255) / 256), 256, 0, s>>>(t->inner[k], to_fe(wm), half, 1);
+    if (k + 1 < p.npass) {
+      const uint64_t total = 1ull << (b + log_J);
+      e = cudaMalloc((void**)&t->twist[k], total * sizeof(fe));
+      if (e != cudaSuccess) return e;
+      t->bytes += total * sizeof(fe);
+      fe *lo = nullptr, *hi = nullptr;
+      uint32_t sh = 0;
+      e = pow_two_level(&lo, &hi, &sh, wMJ, b + log_J, s, true);
+      if (e != cudaSuccess) return e;
+      twist_table_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(t->twist[k], lo, hi, sh, (uint32_t)log_J, total);
+      cudaFreeAsync(lo, s);
+      cudaFreeAsync(hi, s);
+    }
+    done_bits += b;
+  }
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return cudaStreamSynchronize(s);
+}
+
+const NttTables* ntt_tables_get(int device, const host::Fr& omega, int log_n, cudaStream_t s, cudaError_t* err) {
+  Key key{device, log_n, {omega.v[0], omega.v[1], omega.v[2], omega.v[3]}};
+  std::lock_guard<std::mutex> lk(g_mu);
+  auto it = g_cache.find(key);
+  if (it != g_cache.end()) {
+    *err = cudaSuccess;
+    return it->second.get();
+  }
+  auto t = std::make_unique<NttTables>();
+  t->plan = make_ntt_plan(log_n);
+  t->omega = omega;
+  cudaError_t e = build_tables(t.get(), s);
+  if (e != cudaSuccess) {
+    for (int k = 0; k < NTT_MAX_PASS; k++) {
+      if (t->inner[k]) cudaFree(t->inner[k]);
+      if (t->twist[k]) cudaFree(t->twist[k]);
+    }
+    *err = e;
+    return nullptr;
+  }
+  *err = cudaSuccess;
+  const NttTables* res = t.get();
+  g_cache.emplace(key, std::move(t));
+  return res;
+}
+
+template <int B>
+static cudaError_t launch_pass(const PassParams& pp, uint64_t ncta, cudaStream_t s) {
+  constexpr uint32_t M = 1u << B;
+  const uint32_t threads = pp.G * (M / 8);
+  const size_t smem = (size_t)8 * pp.G * M * 4 + (size_t)(M / 2) * 32;
+  static bool attr_set[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr_set[dev & 63]) {
+    cudaFuncSetAttribute(ntt_pass_kernel<B>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr_set[dev & 63] = true;
+  }
+  ntt_pass_kernel<B><<<(unsigned)ncta, threads, smem, s>>>(pp);
+  return cudaGetLastError();
+}
+
+static cudaError_t dispatch_pass(int B, const PassParams& pp, uint64_t ncta, cudaStream_t s) {
+  switch (B) {
+    case 3: return launch_pass<3>(pp, ncta, s);
+    case 4: return launch_pass<4>(pp, ncta, s);
+    case 5: return launch_pass<5>(pp, ncta, s);
+    case 6: return launch_pass<6>(pp, ncta, s);
+    case 7: return launch_pass<7>(pp, ncta, s);
+    case 8: return launch_pass<8>(pp, ncta, s);
+    case 9: return launch_pass<9>(pp, ncta, s);
+    case 10: return launch_pass<10>(pp, ncta, s);
+    case 11: return launch_pass<11>(pp, ncta, s);
+    case 12: return launch_pass<12>(pp, ncta, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t ntt_run(const NttTables& t, fe* d_a, fe* d_tmp, const PowTables* pre, const host::Fr* post, cudaStream_t s) {
+  const NttPlan& p = t.plan;
+  const int L = p.log_n;
+  if (L <= 2) {
+    fe po{};
+    if (post) po = to_fe(*post);
+    ntt_tiny_kernel<<<1, 32, 0, s>>>(d_a, (uint32_t)L, to_fe(t.omega), pre ? pre->lo : nullptr, pre ? pre->hi : nullptr,
+                                     pre ? pre->shift : 0u, post ? 1u : 0u, po);
+    return cudaGetLastError();
+  }
+  int done = 0;
+  for (int k = 0; k < p.npass; k++) {
+    const int b = p.bits[k];
+    const bool final_pass = (k + 1 == p.npass);
+    PassParams pp{};
+    pp.inner = t.inner[k];
+    pp.twist = t.twist[k];
+    pp.log_J = (uint32_t)(L - done - b);
+    pp.log_O = (uint32_t)done;
+    pp.log_m1 = (uint32_t)p.bits[0];
+    pp.nprev = final_pass ? (uint32_t)k : 0u;
+    for (int j = 0; j < k && j < NTT_MAX_PASS; j++) pp.prev_bits[j] = (uint32_t)p.bits[j];
+    pp.is_final = final_pass ? 1u : 0u;
+    if (k == 0 && pre) {
+      pp.pre_lo = pre->lo;
+      pp.pre_hi = pre->hi;
+      pp.pre_shift = pre->shift;
+    }
+    if (final_pass && post) {
+      pp.has_post = 1;
+      pp.post = to_fe(*post);
+    }
+    // buffers: single pass in place; otherwise a -> tmp, tmp in place, tmp -> a
+    if (p.npass == 1) {
+      pp.in = d_a;
+      pp.out = d_a;
+    } else if (k == 0) {
+      pp.in = d_a;
+      pp.out = d_tmp;
+    } else if (!final_pass) {
+      pp.in = d_tmp;
+      pp.out = d_tmp;
+    } else {
+      pp.in = d_tmp;
+      pp.out = d_a;
+    }
+    const uint32_t Gmax = b >= 11 ? 1u : (1u << (11 - b));
+    uint64_t groups_dim;
+    if (!final_pass) {
+      groups_dim = 1ull << pp.log_J;                // columns per outer block
+    } else if (p.npass == 1) {
+      groups_dim = 1;
+    } else {
+      groups_dim = 1ull << p.bits[0];               // consecutive k_1 digits
+    }
+    pp.G = (uint32_t)std::min<uint64_t>(Gmax, groups_dim);
+    const uint64_t total_groups = 1ull << (L - b);
+    const uint64_t ncta = total_groups / pp.G;
+    static const char* names[13] = {"", "", "", "ntt_pass_b3", "ntt_pass_b4", "ntt_pass_b5", "ntt_pass_b6",
+                                    "ntt_pass_b7", "ntt_pass_b8", "ntt_pass_b9", "ntt_pass_b10", "ntt_pass_b11",
+                                    "ntt_pass_b12"};
+    const double nel = (double)(1ull << L);
+    // algorithmic work: radix-2 convention (n/2) * b products; bytes: read + write (+ twist table)
+    ProfScope prof(names[b], s, nel / 2 * b, nel * 32.0 * (final_pass ? 2 : 3));
+    cudaError_t e = dispatch_pass(b, pp, ncta, s);
+    if (e != cudaSuccess) return e;
+    done += b;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t fr_scale_copy(fe* dst, const fe* src, size_t n, size_t dst_stride, const PowTables* powc, cudaStream_t s) {
+  scale_copy_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(dst, src, n, dst_stride, powc ? powc->lo : nullptr,
+                                                               powc ? powc->hi : nullptr, powc ? powc->shift : 0);
+  return cudaGetLastError();
+}
+
+}  // namespace zk

@@ -1,0 +1,77 @@
+// ntt.cuh — Fr number-theoretic transform on sm_100a: plans, device tables,
+// and the launch entry used by the C ABI, the batcher and the LDE pipeline.
+//
+// Algorithm: a natural-order-in / natural-order-out DFT
+//     A[k] = sum_i a[i] * w^(i k)           (w of order exactly n = 2^log_n)
+// computed as a mixed-radix four-step over p passes with bit widths
+// b_1 .. b_p (sum = log_n, each <= 12).  Pass t views the data as
+// [O_t][m_t][J_t] (m_t = 2^b_t, O_t = 2^(b_1+..+b_(t-1)), J_t = 2^(b_(t+1)+..))
+// and runs one m_t-point DIF DFT per (o, j) column, then multiplies output
+// k of column j by the twist w_(m_t J_t)^(k j) and writes it back in place.
+// The last pass writes element (o, k) to rev(o) + (n / m_p) k, where rev
+// reverses o's mixed-radix digits, which lands every A[k] at index k.
+// This replaces the reference's four-step 1024 x n/1024 path
+// (cuda/fft.cu:61-156, 275-405): one kernel per pass instead of five,
+// every thread busy, twiddles from device tables instead of pow_vartime.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstddef>
+
+#include "field.cuh"
+#include "host_field.hpp"
+
+namespace zk {
+
+constexpr int NTT_MAX_LOG = 28;   // Fr two-adicity
+constexpr int NTT_MAX_PASS = 4;
+
+struct NttPlan {
+  int log_n = 0;
+  int npass = 0;
+  int bits[NTT_MAX_PASS] = {0, 0, 0, 0};
+};
+NttPlan make_ntt_plan(int log_n);
+
+// Device tables for one (omega, log_n): per pass the inner roots
+// w_m^e (e < m/2) and, for non-final passes, the twist table [k * J + j].
+struct NttTables {
+  NttPlan plan;
+  host::Fr omega;
+  fe* inner[NTT_MAX_PASS] = {nullptr, nullptr, nullptr, nullptr};
+  fe* twist[NTT_MAX_PASS] = {nullptr, nullptr, nullptr, nullptr};
+  size_t bytes = 0;
+};
+
+// Coset pre-multiplication: input element x is multiplied by c^x, read as
+// lo[x & (2^shift - 1)] * hi[x >> shift].
+struct PowTables {
+  fe* lo = nullptr;
+  fe* hi = nullptr;
+  uint32_t shift = 0;
+};
+
+// Cached tables for (device, omega, log_n); thread-safe.  Returns nullptr and
+// sets *err on failure.  The cache owns the memory.
+const NttTables* ntt_tables_get(int device, const host::Fr& omega, int log_n, cudaStream_t s, cudaError_t* err);
+// Two-level power tables for c^x, x < 2^log_n, allocated from the stream pool
+// (caller frees with pow_tables_free on the same stream).
+cudaError_t pow_tables_make(PowTables* t, const host::Fr& c, int log_n, cudaStream_t s);
+void pow_tables_free(PowTables* t, cudaStream_t s);
+
+// Runs the NTT over d_a (2^log_n elements, in place).  d_tmp is scratch of
+// the same size (unused for single-pass plans).  pre (nullable) applies the
+// coset powers before the transform; post (nullable, host value) scales every
+// output; outputs are canonical.
+cudaError_t ntt_run(const NttTables& t, fe* d_a, fe* d_tmp, const PowTables* pre, const host::Fr* post,
+                    cudaStream_t s);
+
+// Number of launches ntt_run issues for a plan (for launch accounting).
+inline int ntt_launches(const NttPlan& p) { return p.npass; }
+
+// Elementwise helpers used by the LDE pipeline.
+cudaError_t fr_scale_copy(fe* dst, const fe* src, size_t n, size_t dst_stride, const PowTables* powc,
+                          cudaStream_t s);
+
+}  // namespace zk
