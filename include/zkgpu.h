@@ -115,6 +115,18 @@ int zkgpu_ntt_dev(int device, uint64_t *d_a, uint32_t log_n, const uint64_t omeg
 int zkgpu_lagrange_to_extended_dev(int device, const uint64_t *d_values, uint32_t log_n, uint64_t *d_ext,
                                    uint32_t log_ext, const uint64_t omega_inv[4], const uint64_t divisor[4],
                                    const uint64_t g[4], const uint64_t omega_ext[4], void *stream);
+/* No counterpart in the reference.  The same in-place NTT as zkgpu_ntt_dev
+ * (no coset, no scale) for callers that cannot allocate device memory — code
+ * running under stream capture, or inside a runtime that owns every device
+ * allocation.  It calls no allocator: its scratch (ping-pong buffer and root
+ * tables) is a static device array in the library sized for log_n <=
+ * ZKGPU_STATIC_NTT_MAX_LOG (about 16.8 MB per GPU, held until process exit);
+ * larger log_n returns ZKGPU_EINVAL.  The first call on a device resolves the
+ * array's address, so make it before any stream capture starts.  All calls on
+ * a device share the array: calls whose work overlaps on the GPU race and
+ * must be serialised by the caller (one stream or events). */
+#define ZKGPU_STATIC_NTT_MAX_LOG 18
+int zkgpu_ntt_dev_static(int device, uint64_t *d_a, uint32_t log_n, const uint64_t omega[4], void *stream);
 /* d_out_xyz receives the Jacobian sum (12 words, device memory) */
 int zkgpu_msm_dev(int device, const uint64_t *d_scalars, const uint64_t *d_bases_xy, uint64_t n, uint64_t *d_out_xyz,
                   void *stream);

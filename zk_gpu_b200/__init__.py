@@ -65,6 +65,7 @@ EXPORTS = {
     "zkgpu_ntt_dev": (_i32, [_i32, P, _u32, P, P, P, P]),
     "zkgpu_lagrange_to_extended_dev": (_i32, [_i32, P, _u32, P, _u32, P, P, P, P, P]),
     "zkgpu_msm_dev": (_i32, [_i32, P, P, _u64, P, P]),
+    "zkgpu_ntt_dev_static": (_i32, [_i32, P, _u32, P, P]),
     "zkgpu_field_op": (_i32, [_i32, _i32, _i32, P, P, P, _u64]),
     "zkgpu_last_error": (ctypes.c_char_p, []),
     "zkgpu_launch_count": (_u64, [_i32]),

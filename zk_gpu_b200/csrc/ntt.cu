@@ -404,6 +404,61 @@ static cudaError_t build_tables(NttTables* t, cudaStream_t s) {
   return cudaStreamSynchronize(s);
 }
 
+size_t ntt_tables_elems(int log_n) {
+  const NttPlan p = make_ntt_plan(log_n);
+  size_t total = 0;
+  int done = 0;
+  for (int k = 0; k < p.npass; k++) {
+    const int b = p.bits[k];
+    const int log_J = p.log_n - done - b;
+    total += b >= 1 ? (1ull << (b - 1)) : 1;
+    if (k + 1 < p.npass) {
+      const int lc = b + log_J;
+      const int sh = (lc + 1) / 2;
+      total += (1ull << lc) + (1ull << sh) + (1ull << (lc > sh ? lc - sh : 0));
+    }
+    done += b;
+  }
+  return total;
+}
+
+cudaError_t ntt_tables_fill(NttTables* t, const host::Fr& omega, int log_n, fe* mem, size_t cap, cudaStream_t s) {
+  if (ntt_tables_elems(log_n) > cap) return cudaErrorInvalidValue;
+  t->plan = make_ntt_plan(log_n);
+  t->omega = omega;
+  t->bytes = 0;
+  const NttPlan& p = t->plan;
+  fe* cur = mem;
+  int done = 0;
+  for (int k = 0; k < p.npass; k++) {
+    const int b = p.bits[k];
+    const int log_J = p.log_n - done - b;
+    const host::Fr wMJ = host::pow_2k(omega, (unsigned)done);
+    const host::Fr wm = host::pow_2k(wMJ, (unsigned)log_J);
+    const uint64_t half = b >= 1 ? (1ull << (b - 1)) : 1;
+    t->inner[k] = cur;
+    cur += half;
+    pow_seq_kernel<<<(unsigned)((half + 255) / 256), 256, 0, s>>>(t->inner[k], to_fe(wm), half, 1);
+    if (k + 1 < p.npass) {
+      const int lc = b + log_J;
+      const uint32_t sh = (uint32_t)((lc + 1) / 2);
+      const uint64_t total = 1ull << lc, nlo = 1ull << sh, nhi = 1ull << (lc > (int)sh ? lc - sh : 0);
+      fe* lo = cur;
+      fe* hi = cur + nlo;
+      t->twist[k] = cur + nlo + nhi;
+      cur += nlo + nhi + total;
+      pow_seq_kernel<<<(unsigned)((nlo + 255) / 256), 256, 0, s>>>(lo, to_fe(wMJ), nlo, 1);
+      pow_seq_kernel<<<(unsigned)((nhi + 255) / 256), 256, 0, s>>>(hi, to_fe(host::pow_2k(wMJ, sh)), nhi, 1);
+      twist_table_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(t->twist[k], lo, hi, sh, (uint32_t)log_J,
+                                                                          total);
+    } else {
+      t->twist[k] = nullptr;
+    }
+    done += b;
+  }
+  return cudaGetLastError();
+}
+
 const NttTables* ntt_tables_get(int device, const host::Fr& omega, int log_n, cudaStream_t s, cudaError_t* err) {
   Key key{device, log_n, {omega.v[0], omega.v[1], omega.v[2], omega.v[3]}};
   std::lock_guard<std::mutex> lk(g_mu);

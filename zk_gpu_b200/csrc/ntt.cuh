@@ -55,6 +55,10 @@ struct PowTables {
 // Cached tables for (device, omega, log_n); thread-safe.  Returns nullptr and
 // sets *err on failure.  The cache owns the memory.
 const NttTables* ntt_tables_get(int device, const host::Fr& omega, int log_n, cudaStream_t s, cudaError_t* err);
+// Tables for (omega, log_n) written into caller-provided device memory of
+// `cap` elements (no allocation); ntt_tables_elems gives the size needed.
+size_t ntt_tables_elems(int log_n);
+cudaError_t ntt_tables_fill(NttTables* t, const host::Fr& omega, int log_n, fe* mem, size_t cap, cudaStream_t s);
 // Two-level power tables for c^x, x < 2^log_n, allocated from the stream pool
 // (caller frees with pow_tables_free on the same stream).
 cudaError_t pow_tables_make(PowTables* t, const host::Fr& c, int log_n, cudaStream_t s);
