@@ -357,6 +357,61 @@ def _load_peaks():
             pass
 
 
+def run_case(args):
+    """Small single-kernel-family cases for profiler captures (inputs larger
+    than L2, a few hundred MB on the device): `ntt22` = forward NTT of 2^22,
+    `lde20` = LDE 2^20 -> 2^22, `msm20` = MSM of 2^20 points."""
+    import torch
+    import zk_gpu_b200 as zk
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    if args.case in ("ntt22", "lde20"):
+        k = 22 if args.case == "ntt22" else 20
+        c = lde_constants(k, 2)
+        d = torch.from_numpy(rand_fr(1 << k, 7).view(np.int64)).cuda()
+        ext = torch.empty(((1 << (k + 2)), 4), dtype=torch.int64, device="cuda")
+        for _ in range(args.steps):
+            if args.case == "ntt22":
+                zk.ntt_dev(d, k, c["omega"], stream=stream)
+            else:
+                zk.lagrange_to_extended_dev(d, ext, k, k + 2, c["omega_inv"], c["divisor"], c["g"],
+                                            c["omega_ext"], stream=stream)
+    elif args.case == "msm20":
+        n = 1 << 20
+        s = torch.from_numpy(rand_fr(n, 8).view(np.int64)).cuda()
+        b = torch.from_numpy(gen_bases_tiled(n).view(np.int64)).cuda()
+        out = torch.zeros(12, dtype=torch.int64, device="cuda")
+        for _ in range(args.steps):
+            zk.msm_dev(s, b, out, stream=stream)
+    stream.synchronize()
+    print(json.dumps({"case": args.case, "steps": args.steps, "status": "ok"}))
+    return 0
+
+
+def gen_bases_tiled(n: int, distinct: int = 4096) -> np.ndarray:
+    """n affine points: the multiples (i + 1) * G for i < `distinct`, built by
+    repeated addition on the host with Python ints, tiled to length n."""
+    q = 21888242871839275222246405745257275088696311157297823662689037894645226208583
+    d = min(n, distinct)
+    out = np.empty((d, 8), np.uint64)
+    x, y = 1, 2
+    gx, gy = 1, 2
+    rq = (1 << 256) % q
+    m = 2**64 - 1
+    for i in range(d):
+        xm, ym = x * rq % q, y * rq % q
+        out[i] = [(xm >> (64 * j)) & m for j in range(4)] + [(ym >> (64 * j)) & m for j in range(4)]
+        if x == gx:
+            lam = 3 * x * x * pow(2 * y, -1, q) % q
+        else:
+            lam = (gy - y) * pow(gx - x, -1, q) % q
+        x3 = (lam * lam - x - gx) % q
+        y = (lam * (x - x3) - y) % q
+        x = x3
+    reps = (n + d - 1) // d
+    return np.ascontiguousarray(np.tile(out, (reps, 1))[:n])
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -364,11 +419,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--case", choices=["ntt22", "lde20", "msm20"], default=None,
+                    help="run a small profiling case instead of the benchmark")
     args = ap.parse_args()
     _load_peaks()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.case:
+        return run_case(args)
     if args.impl == "reference":
         return run_reference(args, rank, world)
     return run_ours(args, rank, world, local_rank)

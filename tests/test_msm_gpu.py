@@ -1,0 +1,101 @@
+"""GPU parity: the sm_100a Pippenger MSM through the C ABI against the CPU
+oracle (halo2 best_multiexp restated), bit-exact after affine normalisation."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from oracle import bigref as B
+
+pytestmark = pytest.mark.gpu
+
+
+def affine_of(out12):
+    """normalised Jacobian (x, y, one) or all-zero identity -> 8 words (x, y)"""
+    out12 = np.asarray(out12, np.uint64)
+    if not out12[8:12].any():
+        assert not out12.any()
+        return np.zeros(8, np.uint64)
+    return out12[:8].copy()
+
+
+@pytest.mark.parametrize("n", [0, 1, 2, 3, 7, 31, 255, 256, 257, 1000, 4096, 65536])
+def test_msm_sizes(zk, oracle, n):
+    s = oracle.rand_fr(n, 100 + n)
+    pts = oracle.rand_bases(n, 200 + n)
+    got = affine_of(zk.msm(s, pts))
+    assert np.array_equal(got, oracle.multiexp(s, pts))
+
+
+def test_msm_reference_api(zk, oracle):
+    """parallel_msm_api(device, data, GpuAffine*, len, GpuProjective*) (src/api.rs:12)"""
+    n = 1024
+    s = oracle.rand_fr(n, 5)
+    pts = oracle.rand_bases(n, 6)
+    acc = zk.GpuProjective()
+    assert zk.parallel_msm_api(0, s, pts, n, acc) == 0
+    out = np.concatenate([np.array(acc.x, np.uint64), np.array(acc.y, np.uint64), np.array(acc.z, np.uint64)])
+    assert np.array_equal(affine_of(out), oracle.multiexp(s, pts))
+    assert np.array_equal(np.array(acc.z, np.uint64), oracle.to_mont(1, oracle.FQ))
+
+
+def test_msm_edge_cases(zk, oracle):
+    n = 2048
+    pts, k = oracle.rand_bases(n, 9, with_dlog=True)
+    # all-zero scalars -> identity
+    assert not zk.msm(np.zeros((n, 4), np.uint64), pts).any()
+    s = oracle.rand_fr(n, 10)
+    # identity bases (0, 0) are skipped
+    pts2 = pts.copy()
+    pts2[::7] = 0
+    assert np.array_equal(affine_of(zk.msm(s, pts2)), oracle.multiexp(s, pts2))
+    # P + (-P) cancels: scalar 1 and r - 1 on the same base, everything else zero
+    s3 = np.zeros((n, 4), np.uint64)
+    pts3 = pts.copy()
+    pts3[1] = pts3[0]
+    s3[0] = oracle.to_mont(1)
+    s3[1] = oracle.to_mont(B.R_MOD - 1)
+    assert not zk.msm(s3, pts3).any()
+    # the same point many times in one bucket (doubling inside bucket sums)
+    pts4 = np.tile(pts[0], (n, 1))
+    s4 = np.tile(oracle.to_mont(3), (n, 1))
+    assert np.array_equal(affine_of(zk.msm(s4, pts4)), oracle.multiexp(s4, pts4))
+    # extreme scalars: r - 1, 2^253, 2^k - 1 patterns hitting window boundaries
+    vals = [B.R_MOD - 1, 1 << 253, (1 << 254) - 1 - (1 << 200), (1 << 16) - 1, 1 << 15, (1 << 15) + 1, 2**128 - 1]
+    s5 = oracle.rand_fr(n, 11)
+    for i, v in enumerate(vals):
+        s5[i] = oracle.to_mont(v % B.R_MOD)
+    assert np.array_equal(affine_of(zk.msm(s5, pts)), oracle.multiexp(s5, pts))
+
+
+def test_msm_small_scalar_mix(zk, oracle):
+    n = 1 << 16
+    s = oracle.rand_fr(n, 12)
+    small = oracle.rand_fr_small(n // 10, 13, bits=16)
+    s[: n // 10] = small
+    pts, k = oracle.rand_bases(n, 14, with_dlog=True)
+    assert np.array_equal(affine_of(zk.msm(s, pts)), oracle.msm_by_dlog(s, k))
+
+
+def test_msm_full_size_2p22(zk, oracle):
+    """benchmark size: 2^22 bases, 10% scalars < 2^16, checked through the
+    bases' discrete logs: sum s_i [k_i] G = [sum s_i k_i] G"""
+    n = 1 << 22
+    s = oracle.rand_fr(n, 22)
+    s[: n // 10] = oracle.rand_fr_small(n // 10, 23, bits=16)
+    pts, k = oracle.rand_bases(n, 24, with_dlog=True)
+    assert np.array_equal(affine_of(zk.msm(s, pts)), oracle.msm_by_dlog(s, k))
+
+
+def test_msm_device_api(zk, oracle):
+    torch = pytest.importorskip("torch")
+    n = 5000
+    s = oracle.rand_fr(n, 31)
+    pts = oracle.rand_bases(n, 32)
+    ts = torch.from_numpy(s.view(np.int64)).cuda()
+    tb = torch.from_numpy(pts.view(np.int64)).cuda()
+    out = torch.zeros(12, dtype=torch.int64, device="cuda")
+    zk.msm_dev(ts, tb, out)
+    torch.cuda.synchronize()
+    jac = out.cpu().numpy().view(np.uint64)
+    assert np.array_equal(oracle.g1_normalize(jac), oracle.multiexp(s, pts))

@@ -1,8 +1,72 @@
 // api_msm.cu — C-ABI entry points for the G1 MSM (declared in include/zkgpu.h).
+#include <cstring>
+
+#include "host_field.hpp"
+#include "msm.cuh"
 #include "runtime.cuh"
 
-extern "C" uint64_t parallel_msm_api(size_t, const uint64_t*, const GpuAffine*, uint64_t, GpuProjective*) {
-  return ZKGPU_EINVAL;
+using zk::fe;
+
+namespace {
+
+// Host buffers in, normalised Jacobian (12 u64) out.
+int msm_host(int device, const uint64_t* scalars, const uint64_t* bases_xy, uint64_t n, uint64_t out[12]) {
+  if (!out || (n && (!scalars || !bases_xy)) || n >= (1ull << 31)) return ZKGPU_EINVAL;
+  if (n == 0) {
+    std::memset(out, 0, 96);
+    return ZKGPU_OK;
+  }
+  cudaStream_t s;
+  int st = zk::bind_device(device, &s);
+  if (st) return st;
+  fe *ds = nullptr, *db = nullptr, *dout = nullptr;
+  cudaError_t e = cudaMallocAsync((void**)&ds, n * 32, s);
+  if (e == cudaSuccess) e = cudaMallocAsync((void**)&db, n * 64, s);
+  if (e == cudaSuccess) e = cudaMallocAsync((void**)&dout, 96, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(ds, scalars, n * 32, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(db, bases_xy, n * 64, cudaMemcpyHostToDevice, s);
+  uint64_t nl = 0;
+  if (e == cudaSuccess) e = zk::msm_run(ds, db, n, dout, s, 0, &nl);
+  zk::count_launches(nl);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, dout, 96, cudaMemcpyDeviceToHost, s);
+  if (ds) cudaFreeAsync(ds, s);
+  if (db) cudaFreeAsync(db, s);
+  if (dout) cudaFreeAsync(dout, s);
+  cudaError_t e2 = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return zk::status_of("msm", e);
+  if (e2 != cudaSuccess) return zk::status_of("msm sync", e2);
+  zk::host::fq::normalize_jacobian(out);
+  return ZKGPU_OK;
 }
-extern "C" int zkgpu_msm(int, const uint64_t*, const uint64_t*, uint64_t, uint64_t*) { return ZKGPU_EINVAL; }
-extern "C" int zkgpu_msm_dev(int, const uint64_t*, const uint64_t*, uint64_t, uint64_t*, void*) { return ZKGPU_EINVAL; }
+
+}  // namespace
+
+extern "C" uint64_t parallel_msm_api(size_t device_id, const uint64_t* data, const GpuAffine* bases, uint64_t lenght,
+                                     GpuProjective* acc) {
+  if (!acc) return ZKGPU_EINVAL;
+  uint64_t out[12];
+  int st = msm_host((int)device_id, data, reinterpret_cast<const uint64_t*>(bases), lenght, out);
+  if (st) return (uint64_t)st;
+  std::memcpy(acc->x, out, 32);
+  std::memcpy(acc->y, out + 4, 32);
+  std::memcpy(acc->z, out + 8, 32);
+  return ZKGPU_OK;
+}
+
+extern "C" int zkgpu_msm(int device, const uint64_t* scalars, const uint64_t* bases_xy, uint64_t n,
+                         uint64_t out_xyz[12]) {
+  return msm_host(device, scalars, bases_xy, n, out_xyz);
+}
+
+extern "C" int zkgpu_msm_dev(int device, const uint64_t* d_scalars, const uint64_t* d_bases_xy, uint64_t n,
+                             uint64_t* d_out_xyz, void* stream) {
+  if (!d_out_xyz || (n && (!d_scalars || !d_bases_xy)) || n >= (1ull << 31)) return ZKGPU_EINVAL;
+  cudaStream_t own;
+  int st = zk::bind_device(device, &own);
+  if (st) return st;
+  uint64_t nl = 0;
+  cudaError_t e = zk::msm_run(reinterpret_cast<const fe*>(d_scalars), reinterpret_cast<const fe*>(d_bases_xy), n,
+                              reinterpret_cast<fe*>(d_out_xyz), (cudaStream_t)stream, 0, &nl);
+  zk::count_launches(nl);
+  return zk::status_of("msm_dev", e);
+}

@@ -124,5 +124,95 @@ inline bool is_primitive_root(const Fr& w, unsigned log_n) {
   return eq(h, neg(one()));
 }
 
+
+// ---- Fq (base field), used for the MSM's final normalisation -------------
+namespace fq {
+static constexpr uint64_t P[4] = {0x3c208c16d87cfd47ULL, 0x97816a916871ca8dULL, 0xb85045b68181585dULL,
+                                  0x30644e72e131a029ULL};
+static constexpr uint64_t INV = 0x87d20782e4866389ULL;
+static constexpr uint64_t ONE[4] = {0xd35d438dc58f0d9dULL, 0x0a78eb28f5c70b3dULL, 0x666ea36f7879462cULL,
+                                    0x0e0a77c19a07df2fULL};
+struct E {
+  uint64_t v[4];
+};
+inline bool geq_p(const uint64_t a[4]) {
+  for (int i = 3; i >= 0; i--) {
+    if (a[i] != P[i]) return a[i] > P[i];
+  }
+  return true;
+}
+inline void subp(uint64_t a[4]) {
+  unsigned __int128 br = 0;
+  for (int i = 0; i < 4; i++) {
+    unsigned __int128 d = (unsigned __int128)a[i] - P[i] - (uint64_t)br;
+    a[i] = (uint64_t)d;
+    br = (d >> 64) & 1;
+  }
+}
+inline E mul(const E& a, const E& b) {
+  uint64_t t[6] = {0, 0, 0, 0, 0, 0};
+  for (int i = 0; i < 4; i++) {
+    uint64_t c = 0;
+    for (int j = 0; j < 4; j++) {
+      unsigned __int128 s = (unsigned __int128)a.v[j] * b.v[i] + t[j] + c;
+      t[j] = (uint64_t)s;
+      c = (uint64_t)(s >> 64);
+    }
+    unsigned __int128 s = (unsigned __int128)t[4] + c;
+    t[4] = (uint64_t)s;
+    t[5] = (uint64_t)(s >> 64);
+    uint64_t m = t[0] * INV;
+    s = (unsigned __int128)m * P[0] + t[0];
+    c = (uint64_t)(s >> 64);
+    for (int j = 1; j < 4; j++) {
+      s = (unsigned __int128)m * P[j] + t[j] + c;
+      t[j - 1] = (uint64_t)s;
+      c = (uint64_t)(s >> 64);
+    }
+    s = (unsigned __int128)t[4] + c;
+    t[3] = (uint64_t)s;
+    t[4] = t[5] + (uint64_t)(s >> 64);
+  }
+  E r;
+  std::memcpy(r.v, t, sizeof(r.v));
+  if (t[4] || geq_p(r.v)) subp(r.v);
+  return r;
+}
+inline E one() {
+  E r;
+  std::memcpy(r.v, ONE, sizeof(r.v));
+  return r;
+}
+inline bool is_zero(const E& a) { return !(a.v[0] | a.v[1] | a.v[2] | a.v[3]); }
+inline E inv(const E& a) {  // a^(q-2)
+  uint64_t e[4];
+  std::memcpy(e, P, sizeof(e));
+  e[0] -= 2;
+  E r = one();
+  for (int i = 3; i >= 0; i--)
+    for (int b = 63; b >= 0; b--) {
+      r = mul(r, r);
+      if ((e[i] >> b) & 1) r = mul(r, a);
+    }
+  return r;
+}
+// Jacobian (X, Y, Z) -> affine-normalised Jacobian (x, y, one); identity -> zeros
+inline void normalize_jacobian(uint64_t xyz[12]) {
+  E X, Y, Z;
+  std::memcpy(X.v, xyz, 32);
+  std::memcpy(Y.v, xyz + 4, 32);
+  std::memcpy(Z.v, xyz + 8, 32);
+  if (is_zero(Z)) {
+    std::memset(xyz, 0, 96);
+    return;
+  }
+  E zi = inv(Z), zi2 = mul(zi, zi), zi3 = mul(zi2, zi);
+  E x = mul(X, zi2), y = mul(Y, zi3), o = one();
+  std::memcpy(xyz, x.v, 32);
+  std::memcpy(xyz + 4, y.v, 32);
+  std::memcpy(xyz + 8, o.v, 32);
+}
+}  // namespace fq
+
 }  // namespace host
 }  // namespace zk

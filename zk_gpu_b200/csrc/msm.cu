@@ -1,0 +1,290 @@
+// msm.cu — Pippenger MSM kernels and orchestration (see msm.cuh).
+#include <algorithm>
+
+#include "curve.cuh"
+#include "msm.cuh"
+#include "prof.cuh"
+
+namespace zk {
+
+MsmPlan make_msm_plan(uint64_t n, int c_override) {
+  MsmPlan p;
+  int lg = 1;
+  while ((1ull << lg) < n) lg++;
+  int c = lg - 4;
+  if (c < 4) c = 4;
+  if (c > 16) c = 16;
+  if (c_override >= 3 && c_override <= 20) c = c_override;
+  p.c = c;
+  p.windows = (254 + c - 1) / c;
+  p.buckets = 1u << (c - 1);
+  p.seg_len = std::min<uint32_t>(16u, p.buckets);
+  return p;
+}
+
+// bits [pos, pos + c) of a canonical 256-bit scalar (c <= 20), 0 beyond bit 255
+__device__ __forceinline__ uint32_t scalar_bits(const uint32_t s[8], uint32_t pos, uint32_t c) {
+  const uint32_t w = pos >> 5, b = pos & 31;
+  uint64_t v = 0;
+  if (w < 8) v = s[w];
+  if (w + 1 < 8) v |= (uint64_t)s[w + 1] << 32;
+  return (uint32_t)(v >> b) & ((1u << c) - 1u);
+}
+
+// Signed digits of one scalar, low window first; calls f(w, digit) for
+// each non-zero digit (digit in [-2^(c-1), 2^(c-1)]).
+template <class F>
+__device__ __forceinline__ void for_each_digit(const fe* scalar, uint32_t c, uint32_t windows, F f) {
+  uint32_t s[8];
+  ld_fe(s, scalar);
+  uint32_t one[8] = {1, 0, 0, 0, 0, 0, 0, 0};
+  mul<FrP>(s, s, one);  // out of Montgomery form (cuda/curve.cuh:111 does the same)
+  const int half = 1 << (c - 1);
+  uint32_t carry = 0;
+  for (uint32_t w = 0; w < windows; w++) {
+    int v = (int)scalar_bits(s, w * c, c) + (int)carry;
+    if (v > half) {
+      v -= 1 << c;
+      carry = 1;
+    } else {
+      carry = 0;
+    }
+    if (v != 0) f(w, v);
+  }
+}
+
+__global__ void msm_count_kernel(const fe* scalars, uint64_t n, uint32_t c, uint32_t windows, uint32_t* counts) {
+  const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t B = 1u << (c - 1);
+  for_each_digit(scalars + i, c, windows, [&](uint32_t w, int d) {
+    const uint32_t mag = (uint32_t)(d < 0 ? -d : d);
+    atomicAdd(&counts[w * B + mag - 1], 1u);
+  });
+}
+
+__global__ void msm_scatter_kernel(const fe* scalars, uint64_t n, uint32_t c, uint32_t windows, uint32_t* cursor,
+                                   uint32_t* list) {
+  const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t B = 1u << (c - 1);
+  for_each_digit(scalars + i, c, windows, [&](uint32_t w, int d) {
+    const uint32_t mag = (uint32_t)(d < 0 ? -d : d);
+    const uint32_t pos = atomicAdd(&cursor[w * B + mag - 1], 1u);
+    list[pos] = (uint32_t)i | (d < 0 ? 0x80000000u : 0u);
+  });
+}
+
+// Exclusive scan, three phases over 1024-element blocks.
+__global__ void scan_block_kernel(const uint32_t* in, uint32_t* out, uint32_t* block_sums, uint32_t total) {
+  __shared__ uint32_t sh[1024];
+  const uint32_t i = blockIdx.x * 1024 + threadIdx.x;
+  const uint32_t v = i < total ? in[i] : 0;
+  sh[threadIdx.x] = v;
+  __syncthreads();
+  for (uint32_t off = 1; off < 1024; off <<= 1) {
+    uint32_t t = threadIdx.x >= off ? sh[threadIdx.x - off] : 0;
+    __syncthreads();
+    sh[threadIdx.x] += t;
+    __syncthreads();
+  }
+  if (i < total) out[i] = sh[threadIdx.x] - v;
+  if (threadIdx.x == 1023) block_sums[blockIdx.x] = sh[1023];
+}
+__global__ void scan_sums_kernel(uint32_t* block_sums, uint32_t nblocks, uint32_t* total_out) {
+  // one block of 1024 threads; nblocks <= 1024 * 64
+  __shared__ uint32_t sh[1024];
+  uint32_t carry = 0;
+  for (uint32_t base = 0; base < nblocks; base += 1024) {
+    const uint32_t i = base + threadIdx.x;
+    const uint32_t v = i < nblocks ? block_sums[i] : 0;
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (uint32_t off = 1; off < 1024; off <<= 1) {
+      uint32_t t = threadIdx.x >= off ? sh[threadIdx.x - off] : 0;
+      __syncthreads();
+      sh[threadIdx.x] += t;
+      __syncthreads();
+    }
+    if (i < nblocks) block_sums[i] = carry + sh[threadIdx.x] - v;
+    const uint32_t tot = sh[1023];
+    __syncthreads();
+    carry += tot;
+  }
+  if (threadIdx.x == 0) *total_out = carry;
+}
+__global__ void scan_add_kernel(uint32_t* out, uint32_t* cursor, const uint32_t* block_sums, uint32_t total) {
+  const uint32_t i = blockIdx.x * 1024 + threadIdx.x;
+  if (i >= total) return;
+  const uint32_t v = out[i] + block_sums[blockIdx.x];
+  out[i] = v;
+  cursor[i] = v;
+}
+
+// One thread per bucket: sum of its (signed) points.
+__global__ void __launch_bounds__(256) msm_bucket_kernel(const uint32_t* list, const uint32_t* offsets,
+                                                         const uint32_t* counts, const fe* bases, fe* buckets,
+                                                         uint32_t total_buckets) {
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= total_buckets) return;
+  const uint32_t beg = offsets[b], cnt = counts[b];
+  xyzz_t acc;
+  xyzz_set_inf(acc);
+  for (uint32_t k = 0; k < cnt; k++) {
+    const uint32_t e = list[beg + k];
+    aff_t q;
+    ld_aff(q, bases + 2 * (uint64_t)(e & 0x7fffffffu));
+    if (aff_is_inf(q)) continue;
+    if (e & 0x80000000u) {
+      uint32_t z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      sub<FqP>(q.y, z, q.y);
+    }
+    xyzz_madd(acc, q);
+  }
+  st_xyzz(buckets + 4 * (uint64_t)b, acc);
+}
+
+// Per (window, segment): running sums over the segment's buckets, top down,
+// giving sum_j (j - lo + 1) B_j and sum_j B_j; result T + lo * S, which is
+// the segment's share of sum_j (j + 1) B_j.
+__global__ void __launch_bounds__(128) msm_segment_kernel(const fe* buckets, fe* segres, uint32_t B, uint32_t L,
+                                                          uint32_t total_segs) {
+  const uint32_t gs = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gs >= total_segs) return;
+  const uint32_t S_per_w = B / L;
+  const uint32_t w = gs / S_per_w, s = gs % S_per_w;
+  const uint32_t lo = s * L;
+  xyzz_t run, tot, bk;
+  xyzz_set_inf(run);
+  xyzz_set_inf(tot);
+  for (int j = (int)(lo + L) - 1; j >= (int)lo; j--) {
+    ld_xyzz(bk, buckets + 4 * ((uint64_t)w * B + j));
+    xyzz_add(run, bk);
+    xyzz_add(tot, run);
+  }
+  xyzz_mul_small(run, lo);
+  xyzz_add(tot, run);
+  st_xyzz(segres + 4 * (uint64_t)gs, tot);
+}
+
+// One block per window: tree sum of its segment results.
+__global__ void __launch_bounds__(256) msm_window_kernel(const fe* segres, fe* winsum, uint32_t S_per_w) {
+  __shared__ fe sh[256 * 4];
+  const uint32_t w = blockIdx.x;
+  xyzz_t acc, t;
+  xyzz_set_inf(acc);
+  for (uint32_t s = threadIdx.x; s < S_per_w; s += blockDim.x) {
+    ld_xyzz(t, segres + 4 * ((uint64_t)w * S_per_w + s));
+    xyzz_add(acc, t);
+  }
+  st_xyzz(sh + 4 * threadIdx.x, acc);
+  __syncthreads();
+  for (uint32_t half = blockDim.x / 2; half > 0; half >>= 1) {
+    if (threadIdx.x < half) {
+      ld_xyzz(acc, sh + 4 * threadIdx.x);
+      ld_xyzz(t, sh + 4 * (threadIdx.x + half));
+      xyzz_add(acc, t);
+      st_xyzz(sh + 4 * threadIdx.x, acc);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    ld_xyzz(acc, sh);
+    st_xyzz(winsum + 4 * (uint64_t)w, acc);
+  }
+}
+
+// Horner over windows (high to low) and conversion to Jacobian.
+__global__ void msm_combine_kernel(const fe* winsum, uint32_t windows, uint32_t c, fe* out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  xyzz_t acc, t;
+  ld_xyzz(acc, winsum + 4 * (uint64_t)(windows - 1));
+  for (int w = (int)windows - 2; w >= 0; w--) {
+    for (uint32_t k = 0; k < c; k++) xyzz_dbl(acc, acc);
+    ld_xyzz(t, winsum + 4 * (uint64_t)w);
+    xyzz_add(acc, t);
+  }
+  uint32_t j[24];
+  xyzz_to_jacobian(j, acc);
+  st_fe(out, j);
+  st_fe(out + 1, j + 8);
+  st_fe(out + 2, j + 16);
+}
+
+__global__ void zero_out_kernel(fe* out) {
+  if (threadIdx.x < 3) {
+    uint32_t z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    st_fe(out + threadIdx.x, z);
+  }
+}
+
+cudaError_t msm_run(const fe* d_scalars, const fe* d_bases, uint64_t n, fe* d_out, cudaStream_t s, int c_override,
+                    uint64_t* launches) {
+  uint64_t nl = 0;
+  if (n == 0) {
+    zero_out_kernel<<<1, 32, 0, s>>>(d_out);
+    if (launches) *launches = 1;
+    return cudaGetLastError();
+  }
+  const MsmPlan p = make_msm_plan(n, c_override);
+  const uint32_t W = (uint32_t)p.windows, B = p.buckets, L = p.seg_len;
+  const uint32_t total = W * B;
+  const uint32_t nblk = (total + 1023) / 1024;
+  const uint64_t entries = n * (uint64_t)W;
+  uint32_t *counts = nullptr, *offsets = nullptr, *cursor = nullptr, *bsums = nullptr, *list = nullptr;
+  fe *buckets = nullptr, *segres = nullptr, *winsum = nullptr;
+  const uint32_t segs = total / L;
+  cudaError_t e = cudaSuccess;
+  auto alloc = [&](void** ptr, size_t bytes) {
+    if (e == cudaSuccess) e = cudaMallocAsync(ptr, bytes, s);
+  };
+  alloc((void**)&counts, total * 4ull);
+  alloc((void**)&offsets, (total + 1) * 4ull);
+  alloc((void**)&cursor, total * 4ull);
+  alloc((void**)&bsums, (nblk + 1) * 4ull);
+  alloc((void**)&list, entries * 4ull);
+  alloc((void**)&buckets, total * 128ull);
+  alloc((void**)&segres, segs * 128ull);
+  alloc((void**)&winsum, W * 128ull);
+  if (e == cudaSuccess) {
+    const double nd = (double)n;
+    cudaMemsetAsync(counts, 0, total * 4ull, s);
+    const unsigned g = (unsigned)((n + 255) / 256);
+    {
+      ProfScope ps("msm_count", s, nd, nd * 32);
+      msm_count_kernel<<<g, 256, 0, s>>>(d_scalars, n, (uint32_t)p.c, W, counts);
+    }
+    scan_block_kernel<<<nblk, 1024, 0, s>>>(counts, offsets, bsums, total);
+    scan_sums_kernel<<<1, 1024, 0, s>>>(bsums, nblk, offsets + total);
+    scan_add_kernel<<<nblk, 1024, 0, s>>>(offsets, cursor, bsums, total);
+    {
+      ProfScope ps("msm_scatter", s, nd, nd * 32 + (double)entries * 4);
+      msm_scatter_kernel<<<g, 256, 0, s>>>(d_scalars, n, (uint32_t)p.c, W, cursor, list);
+    }
+    {
+      // convention: 6 Fq products per point-window (batch-affine cost)
+      ProfScope ps("msm_bucket", s, (double)entries * 6, (double)entries * (64 + 4) + total * 128.0);
+      msm_bucket_kernel<<<(total + 255) / 256, 256, 0, s>>>(list, offsets, counts, d_bases, buckets, total);
+    }
+    {
+      ProfScope ps("msm_segment", s, (double)total * 2 * 14, total * 128.0);
+      msm_segment_kernel<<<(segs + 127) / 128, 128, 0, s>>>(buckets, segres, B, L, segs);
+    }
+    msm_window_kernel<<<W, 256, 0, s>>>(segres, winsum, B / L);
+    msm_combine_kernel<<<1, 32, 0, s>>>(winsum, W, (uint32_t)p.c, d_out);
+    nl = 9;
+    e = cudaGetLastError();
+  }
+  if (counts) cudaFreeAsync(counts, s);
+  if (offsets) cudaFreeAsync(offsets, s);
+  if (cursor) cudaFreeAsync(cursor, s);
+  if (bsums) cudaFreeAsync(bsums, s);
+  if (list) cudaFreeAsync(list, s);
+  if (buckets) cudaFreeAsync(buckets, s);
+  if (segres) cudaFreeAsync(segres, s);
+  if (winsum) cudaFreeAsync(winsum, s);
+  if (launches) *launches = nl;
+  return e;
+}
+
+}  // namespace zk

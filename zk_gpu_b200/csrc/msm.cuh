@@ -1,0 +1,38 @@
+// msm.cuh — G1 multi-scalar multiplication (Pippenger) on sm_100a.
+//
+//   sum_i s_i * P_i,  s_i in Fr (Montgomery), P_i affine in Fq (Montgomery)
+//
+// This replaces the reference's one-thread-per-chunk serial Pippenger with
+// local-memory buckets (cuda/fft.cu:158-221, 450-551):
+//   1. digits   : every scalar -> W signed c-bit digits d_w in
+//                 [-2^(c-1), 2^(c-1)]; each non-zero digit is an entry
+//                 (bucket = w * 2^(c-1) + |d_w| - 1, point index, sign).
+//   2. sort     : counting sort of the entries by bucket (histogram, scan,
+//                 scatter), so each bucket's points are contiguous.
+//   3. buckets  : one thread per bucket sums its points (XYZZ mixed adds).
+//   4. reduce   : per window, sum_b b * B_b by segmented running sums
+//                 (segment results T_s + lo_s * S_s), then a block tree sum.
+//   5. combine  : Horner over windows, sum_w 2^(c w) W_w, as Jacobian.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "field.cuh"
+
+namespace zk {
+
+struct MsmPlan {
+  int c = 0;         // window bits
+  int windows = 0;   // W
+  uint32_t buckets = 0;  // per window, 2^(c-1)
+  uint32_t seg_len = 0;  // buckets per reduction segment
+};
+MsmPlan make_msm_plan(uint64_t n, int c_override = 0);
+
+// Enqueue the MSM on `s`; d_out receives the Jacobian sum (X, Y, Z: 12 u64,
+// not normalised; identity = Z 0).  Scratch comes from the stream pool.
+cudaError_t msm_run(const fe* d_scalars, const fe* d_bases_xy, uint64_t n, fe* d_out, cudaStream_t s,
+                    int c_override = 0, uint64_t* launches = nullptr);
+
+}  // namespace zk
