@@ -278,6 +278,28 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     ntt_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
     del d_a
 
+    # ---- MSM 2^22 (sub-metric): 10% of scalars < 2^16, resident bases ----
+    n_msm = 1 << 22
+    sc = rand_fr(n_msm, 4242 + rank)
+    sc[: n_msm // 10] = small_fr(n_msm // 10, 4343 + rank)
+    d_sc = torch.from_numpy(sc.view(np.int64)).to(f"cuda:{dev}")
+    d_bs = torch.from_numpy(gen_bases_tiled(n_msm).view(np.int64)).to(f"cuda:{dev}")
+    d_out = torch.zeros(12, dtype=torch.int64, device=f"cuda:{dev}")
+    zk.msm_dev(d_sc, d_bs, d_out, stream=stream)
+    stream.synchronize()
+    msm_steps = max(3, min(args.steps, 10))
+    zk.prof_reset()
+    zk.prof_enable(True)
+    e0.record(stream)
+    for _ in range(msm_steps):
+        zk.msm_dev(d_sc, d_bs, d_out, stream=stream)
+    e1.record(stream)
+    stream.synchronize()
+    zk.prof_enable(False)
+    msm_prof = zk.prof_read()
+    msm_ms = max_over_ranks(e0.elapsed_time(e1) / msm_steps)
+    del d_sc, d_bs
+
     # ---- e2e through the host-buffer C ABI, pinned host memory ----
     h_vals = torch.from_numpy(vals_np.view(np.int64)).pin_memory()
     h_ext = torch.empty((N, 4), dtype=torch.int64).pin_memory()
@@ -327,7 +349,11 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "roofline": roof,
         "kernels": {k: {"launches": v["launches"], "ms": round(v["ms"], 3)} for k, v in prof.items()},
         "extra": {"ntt_fwd_2p24_melem_s": round(world * n / (ntt_ms * 1e-3) / 1e6, 2),
-                  "ntt_fwd_2p24_ms": round(ntt_ms, 4)},
+                  "ntt_fwd_2p24_ms": round(ntt_ms, 4),
+                  "msm_2p22_mpts_s": round(world * n_msm / (msm_ms * 1e-3) / 1e6, 2),
+                  "msm_2p22_ms": round(msm_ms, 3),
+                  "msm_kernels": {k: {"launches": v["launches"], "ms": round(v["ms"], 3)} for k, v in msm_prof.items()},
+                  "msm_roofline": msm_roofline(msm_prof, imad_ps, n_msm, msm_ms)},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         t, threads = cpu_lde_sample()
@@ -341,6 +367,32 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def small_fr(n: int, seed: int, bits: int = 16) -> np.ndarray:
+    """n uniform canonical values < 2^bits, in Montgomery form"""
+    rng = np.random.default_rng(seed)
+    vals = rng.integers(0, 1 << bits, size=n, dtype=np.uint64)
+    out = np.empty((n, 4), np.uint64)
+    m = 2**64 - 1
+    for i, v in enumerate(vals.tolist()):
+        x = v * MONT_R % R_MOD
+        out[i] = [(x >> (64 * j)) & m for j in range(4)]
+    return out
+
+
+def msm_roofline(prof: dict, imad_ps: float, n: int, total_ms: float):
+    """Whole-MSM roofline: fixed work convention 16 windows x 1 bucket add per
+    point x 6 Fq products (batch-affine cost) x 256 IMAD per product."""
+    work = n * 16 * 6
+    achieved = work * 256 / (total_ms * 1e-3)
+    out = {"bound": "imad", "achieved": round(achieved / 1e12, 3), "peak": round(imad_ps / 1e12, 3),
+           "unit": "TIMAD/s", "frac": round(achieved / imad_ps, 4), "work_fq_products": work}
+    b = prof.get("msm_bucket")
+    if b:
+        out["bucket_kernel_ms_per_launch"] = round(b["ms"] / b["launches"], 3)
+        out["bucket_kernel_share"] = round(b["ms"] / sum(v["ms"] for v in prof.values()), 3)
+    return out
 
 
 HBM_GBS = 6543.1
@@ -365,13 +417,15 @@ def run_case(args):
     import zk_gpu_b200 as zk
     torch.cuda.set_device(0)
     stream = torch.cuda.Stream()
-    if args.case in ("ntt22", "lde20"):
-        k = 22 if args.case == "ntt22" else 20
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if args.case in ("ntt22", "lde20", "ntt24"):
+        k = {"ntt22": 22, "lde20": 20, "ntt24": 24}[args.case]
         c = lde_constants(k, 2)
         d = torch.from_numpy(rand_fr(1 << k, 7).view(np.int64)).cuda()
-        ext = torch.empty(((1 << (k + 2)), 4), dtype=torch.int64, device="cuda")
-        for _ in range(args.steps):
-            if args.case == "ntt22":
+        ext = torch.empty(((1 << (k + 2)), 4), dtype=torch.int64, device="cuda") if args.case == "lde20" else None
+
+        def step():
+            if ext is None:
                 zk.ntt_dev(d, k, c["omega"], stream=stream)
             else:
                 zk.lagrange_to_extended_dev(d, ext, k, k + 2, c["omega_inv"], c["divisor"], c["g"],
@@ -381,10 +435,18 @@ def run_case(args):
         s = torch.from_numpy(rand_fr(n, 8).view(np.int64)).cuda()
         b = torch.from_numpy(gen_bases_tiled(n).view(np.int64)).cuda()
         out = torch.zeros(12, dtype=torch.int64, device="cuda")
-        for _ in range(args.steps):
+
+        def step():
             zk.msm_dev(s, b, out, stream=stream)
+    step()
     stream.synchronize()
-    print(json.dumps({"case": args.case, "steps": args.steps, "status": "ok"}))
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    stream.synchronize()
+    print(json.dumps({"case": args.case, "steps": args.steps, "status": "ok",
+                      "ms_per_step": round(e0.elapsed_time(e1) / args.steps, 4)}))
     return 0
 
 
@@ -419,7 +481,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--case", choices=["ntt22", "lde20", "msm20"], default=None,
+    ap.add_argument("--case", choices=["ntt22", "ntt24", "lde20", "msm20"], default=None,
                     help="run a small profiling case instead of the benchmark")
     args = ap.parse_args()
     _load_peaks()

@@ -21,39 +21,21 @@ namespace zk {
 // ---------------------------------------------------------------------------
 // integer-pipe peak
 // ---------------------------------------------------------------------------
-// 8 independent (lo, hi) multiply-add chains per thread; each asm block is
-// 16 IMAD-class instructions (8 mad.lo.cc + 8 madc.hi.cc, one carry chain).
+// 8 independent 32-bit multiply-add chains per thread (c = c * a + b, each
+// step depends on the last, so nothing is hoisted); one IMAD per step.  This
+// is the integer pipe's issue peak (64 per SM-clock on sm_100), the
+// conservative denominator: carry-chained forms (madc.hi) run slower.
 __global__ void imad_peak_kernel(uint32_t* sink, uint32_t iters, uint32_t seed) {
   uint32_t a[8], c[8];
 #pragma unroll
   for (int i = 0; i < 8; i++) {
-    a[i] = seed * (threadIdx.x + 3 * i + 1);
+    a[i] = (seed * (threadIdx.x + 3 * i + 1)) | 1u;
     c[i] = seed ^ (blockIdx.x * 77u + i);
   }
   const uint32_t b = seed | 1u;
   for (uint32_t it = 0; it < iters; it++) {
-    asm volatile(
-        "mad.lo.cc.u32  %0, %8, %16, %0;\n\t"
-        "madc.hi.cc.u32 %1, %9, %16, %1;\n\t"
-        "madc.lo.cc.u32 %2, %10, %16, %2;\n\t"
-        "madc.hi.cc.u32 %3, %11, %16, %3;\n\t"
-        "madc.lo.cc.u32 %4, %12, %16, %4;\n\t"
-        "madc.hi.cc.u32 %5, %13, %16, %5;\n\t"
-        "madc.lo.cc.u32 %6, %14, %16, %6;\n\t"
-        "madc.hi.u32    %7, %15, %16, %7;\n\t"
-        : "+r"(c[0]), "+r"(c[1]), "+r"(c[2]), "+r"(c[3]), "+r"(c[4]), "+r"(c[5]), "+r"(c[6]), "+r"(c[7])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]), "r"(b));
-    asm volatile(
-        "mad.lo.cc.u32  %0, %8, %16, %0;\n\t"
-        "madc.hi.cc.u32 %1, %9, %16, %1;\n\t"
-        "madc.lo.cc.u32 %2, %10, %16, %2;\n\t"
-        "madc.hi.cc.u32 %3, %11, %16, %3;\n\t"
-        "madc.lo.cc.u32 %4, %12, %16, %4;\n\t"
-        "madc.hi.cc.u32 %5, %13, %16, %5;\n\t"
-        "madc.lo.cc.u32 %6, %14, %16, %6;\n\t"
-        "madc.hi.u32    %7, %15, %16, %7;\n\t"
-        : "+r"(a[0]), "+r"(a[1]), "+r"(a[2]), "+r"(a[3]), "+r"(a[4]), "+r"(a[5]), "+r"(a[6]), "+r"(a[7])
-        : "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(c[4]), "r"(c[5]), "r"(c[6]), "r"(c[7]), "r"(b));
+#pragma unroll
+    for (int i = 0; i < 8; i++) c[i] = c[i] * a[i] + b;
   }
   uint32_t acc = 0;
 #pragma unroll
@@ -72,7 +54,7 @@ __global__ void modmul_rate_kernel(uint32_t* sink, uint32_t iters, uint32_t seed
   }
   for (uint32_t it = 0; it < iters; it++) {
 #pragma unroll
-    for (int k = 0; k < 4; k++) mul_lazy<FrP>(x[k], x[k], y);
+    for (int k = 0; k < 4; k++) mul_r29<FrP>(x[k], x[k], y);
   }
   uint32_t acc = 0;
 #pragma unroll
@@ -149,7 +131,7 @@ extern "C" int zkgpu_int_peak(int device, uint32_t iters, double* imad_per_s, do
   cudaEventSynchronize(e1);
   float ms = 0;
   cudaEventElapsedTime(&ms, e0, e1);
-  if (imad_per_s) *imad_per_s = (double)blocks * threads * iters * 32.0 / (ms * 1e-3);
+  if (imad_per_s) *imad_per_s = (double)blocks * threads * iters * 8.0 / (ms * 1e-3);
   const uint32_t mm_iters = iters / 16 > 0 ? iters / 16 : 1;
   zk::modmul_rate_kernel<<<blocks, threads, 0, s>>>(sink, 4, 777u);
   cudaEventRecord(e0, s);

@@ -34,6 +34,9 @@ struct FrP {
   // R mod p (Montgomery one)
   static constexpr uint32_t O0 = 0x4ffffffbu, O1 = 0xac96341cu, O2 = 0x9f60cd29u, O3 = 0x36fc7695u,
                             O4 = 0x7879462eu, O5 = 0x666ea36fu, O6 = 0x9a07df2fu, O7 = 0x0e0a77c1u;
+  // 2^261 mod p (the one of the R' = 2^261 form used by mul_r29)
+  static constexpr uint32_t Q0 = 0x8fffff57u, Q1 = 0x2fd4e156u, Q2 = 0xa494b01au, Q3 = 0x75bba827u,
+                            Q4 = 0x819caa80u, Q5 = 0x5301fa84u, Q6 = 0x563d4475u, Q7 = 0x0dc83629u;
 };
 struct FqP {
   static constexpr uint32_t P0 = 0xd87cfd47u, P1 = 0x3c208c16u, P2 = 0x6871ca8du, P3 = 0x97816a91u,
@@ -41,6 +44,8 @@ struct FqP {
   static constexpr uint32_t INV = 0xe4866389u;
   static constexpr uint32_t O0 = 0xc58f0d9du, O1 = 0xd35d438du, O2 = 0xf5c70b3du, O3 = 0x0a78eb28u,
                             O4 = 0x7879462cu, O5 = 0x666ea36fu, O6 = 0x9a07df2fu, O7 = 0x0e0a77c1u;
+  static constexpr uint32_t Q0 = 0x157ccc21u, Q1 = 0x4e8384ebu, Q2 = 0x0ce148c3u, Q3 = 0xfb90a602u,
+                            Q4 = 0x819caa36u, Q5 = 0x5301fa84u, Q6 = 0x563d4475u, Q7 = 0x0dc83629u;
 };
 
 #define ZK_P_OPS(P) "n"(P::INV), "n"(P::P0), "n"(P::P1), "n"(P::P2), "n"(P::P3), "n"(P::P4), "n"(P::P5), "n"(P::P6), "n"(P::P7)
@@ -323,6 +328,112 @@ __device__ __forceinline__ void pow_u64(uint32_t r[8], const uint32_t a[8], uint
     if (e) sqr<P>(base, base);
   }
   cpy(r, acc);
+}
+
+// ---- reduced-radix Montgomery product (9 limbs of 29 bits, R' = 2^261) ----
+// Products of 29-bit limbs are < 2^58, so a 64-bit column accumulator takes
+// every partial product of a column (at most 18, < 2^62.2) through one
+// mad.wide.u32 each, with no carry chain; carries are resolved once per
+// row (T[i+1] += T[i] >> 29).  It computes a*b*2^-261 mod p, so one operand
+// is kept in "R' form" (x * 2^261 mod p): R-form data (x * 2^256) times an
+// R'-form constant gives R-form data.  Inputs < 2p give a result < 2p
+// (4p^2 / 2^261 < p / 32).
+constexpr uint32_t M29 = (1u << 29) - 1;
+
+__device__ __forceinline__ void split29(uint32_t l[9], const uint32_t a[8]) {
+  l[0] = a[0] & M29;
+  l[1] = __funnelshift_r(a[0], a[1], 29) & M29;
+  l[2] = __funnelshift_r(a[1], a[2], 26) & M29;
+  l[3] = __funnelshift_r(a[2], a[3], 23) & M29;
+  l[4] = __funnelshift_r(a[3], a[4], 20) & M29;
+  l[5] = __funnelshift_r(a[4], a[5], 17) & M29;
+  l[6] = __funnelshift_r(a[5], a[6], 14) & M29;
+  l[7] = __funnelshift_r(a[6], a[7], 11) & M29;
+  l[8] = a[7] >> 8;
+}
+
+__device__ __forceinline__ void pack29(uint32_t w[8], const uint32_t l[9]) {
+  w[0] = l[0] | (l[1] << 29);
+  w[1] = (l[1] >> 3) | (l[2] << 26);
+  w[2] = (l[2] >> 6) | (l[3] << 23);
+  w[3] = (l[3] >> 9) | (l[4] << 20);
+  w[4] = (l[4] >> 12) | (l[5] << 17);
+  w[5] = (l[5] >> 15) | (l[6] << 14);
+  w[6] = (l[6] >> 18) | (l[7] << 11);
+  w[7] = (l[7] >> 21) | (l[8] << 8);
+}
+
+// 29-bit limb j of the modulus, and -p^-1 mod 2^29
+template <class P>
+__host__ __device__ constexpr uint32_t p29(int j) {
+  return j == 0   ? (P::P0 & M29)
+         : j == 1 ? (((P::P0 >> 29) | (P::P1 << 3)) & M29)
+         : j == 2 ? (((P::P1 >> 26) | (P::P2 << 6)) & M29)
+         : j == 3 ? (((P::P2 >> 23) | (P::P3 << 9)) & M29)
+         : j == 4 ? (((P::P3 >> 20) | (P::P4 << 12)) & M29)
+         : j == 5 ? (((P::P4 >> 17) | (P::P5 << 15)) & M29)
+         : j == 6 ? (((P::P5 >> 14) | (P::P6 << 18)) & M29)
+         : j == 7 ? (((P::P6 >> 11) | (P::P7 << 21)) & M29)
+                  : (P::P7 >> 8);
+}
+template <class P>
+__host__ __device__ constexpr uint32_t inv29() {
+  return P::INV & M29;  // -p^-1 mod 2^32 reduced mod 2^29
+}
+
+// r = a * b' * 2^-261 mod p, limbs given pre-split (al, bl < 2^29 each,
+// values < 2p); result as 9 normalised limbs.
+template <class P>
+__device__ __forceinline__ void mul29_limbs(uint32_t rl[9], const uint32_t al[9], const uint32_t bl[9]) {
+  uint64_t T[17];
+#pragma unroll
+  for (int k = 0; k < 17; k++) T[k] = 0;
+#pragma unroll
+  for (int i = 0; i < 9; i++) {
+#pragma unroll
+    for (int j = 0; j < 9; j++) T[i + j] += (uint64_t)al[j] * bl[i];
+    const uint32_t m = ((uint32_t)T[i] * inv29<P>()) & M29;
+#pragma unroll
+    for (int j = 0; j < 9; j++) T[i + j] += (uint64_t)m * p29<P>(j);
+    T[i + 1] += T[i] >> 29;
+  }
+  uint64_t c = 0;
+#pragma unroll
+  for (int k = 9; k < 17; k++) {
+    const uint64_t v = T[k] + c;
+    rl[k - 9] = (uint32_t)v & M29;
+    c = v >> 29;
+  }
+  rl[8] = (uint32_t)c;
+}
+
+// 8-word interface: r = a * b' * 2^-261 (b' in R' form), lazy (< 2p).
+template <class P>
+__device__ __forceinline__ void mul_r29(uint32_t r[8], const uint32_t a[8], const uint32_t b[8]) {
+  uint32_t al[9], bl[9], rl[9];
+  split29(al, a);
+  split29(bl, b);
+  mul29_limbs<P>(rl, al, bl);
+  pack29(r, rl);
+}
+
+template <class P>
+__device__ __forceinline__ void set_one_r29(uint32_t r[8]) {
+  r[0] = P::Q0; r[1] = P::Q1; r[2] = P::Q2; r[3] = P::Q3;
+  r[4] = P::Q4; r[5] = P::Q5; r[6] = P::Q6; r[7] = P::Q7;
+}
+// a^e with a and the result in R' form (canonical)
+template <class P>
+__device__ __forceinline__ void pow_u64_r29(uint32_t r[8], const uint32_t a[8], uint64_t e) {
+  uint32_t acc[8], base[8];
+  set_one_r29<P>(acc);
+  cpy(base, a);
+  while (e) {
+    if (e & 1) mul_r29<P>(acc, acc, base);
+    e >>= 1;
+    if (e) mul_r29<P>(base, base, base);
+  }
+  reduce_once<P>(r, acc);
 }
 
 // ---- global memory element access (32 B = one sector, two 16 B vectors) --

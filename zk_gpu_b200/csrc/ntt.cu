@@ -90,13 +90,13 @@ __device__ __forceinline__ void ntt_round(uint32_t x[8][8], uint32_t q, const ui
         } else {
           uint32_t w[8];
           ld_smem_fe(w, tws, HALF, e);
-          mul_lazy<P_r>(x[r2], t, w);
+          mul_r29<P_r>(x[r2], t, w);
         }
       } else {
         const uint32_t e = ((q & ((1u << LO) - 1u)) | ((uint32_t)(r & ((1 << rb) - 1)) << LO)) << (B - 1 - b);
         uint32_t w[8];
         ld_smem_fe(w, tws, HALF, e);
-        mul_lazy<P_r>(x[r2], t, w);
+        mul_r29<P_r>(x[r2], t, w);
       }
     }
   }
@@ -144,8 +144,11 @@ struct PassParams {
   fe post;
 };
 
+#ifndef ZK_NTT_MIN_BLOCKS
+#define ZK_NTT_MIN_BLOCKS 2
+#endif
 template <int B>
-__global__ void __launch_bounds__(B >= 12 ? 512 : 256, B >= 12 ? 1 : 2) ntt_pass_kernel(const PassParams p) {
+__global__ void __launch_bounds__(B >= 12 ? 512 : 256, B >= 12 ? 1 : ZK_NTT_MIN_BLOCKS) ntt_pass_kernel(const PassParams p) {
   constexpr uint32_t M = 1u << B;
   constexpr uint32_t T = M / 8;  // threads per column
   extern __shared__ uint32_t smem[];
@@ -191,8 +194,8 @@ __global__ void __launch_bounds__(B >= 12 ? 512 : 256, B >= 12 ? 1 : 2) ntt_pass
       uint32_t a[8], b[8];
       ld_fe_nc(a, p.pre_lo + (xi & mask));
       ld_fe_nc(b, p.pre_hi + (xi >> p.pre_shift));
-      mul_lazy<P_r>(a, a, b);
-      mul_lazy<P_r>(x[r], x[r], a);
+      mul_r29<P_r>(a, a, b);
+      mul_r29<P_r>(x[r], x[r], a);
     }
   }
   __syncthreads();
@@ -206,7 +209,7 @@ __global__ void __launch_bounds__(B >= 12 ? 512 : 256, B >= 12 ? 1 : 2) ntt_pass
       const uint32_t k = __brev(8 * q + r) >> (32 - B);
       uint32_t w[8];
       ld_fe_nc(w, p.twist + (uint64_t)k * J + col);
-      mul_lazy<P_r>(x[r], x[r], w);
+      mul_r29<P_r>(x[r], x[r], w);
       st_fe(p.out + o * (uint64_t)M * J + (uint64_t)k * J + col, x[r]);
     }
   } else {
@@ -232,7 +235,7 @@ __global__ void __launch_bounds__(B >= 12 ? 512 : 256, B >= 12 ? 1 : 2) ntt_pass
       const uint32_t k = __brev(8 * q + r) >> (32 - B);
       uint32_t v[8];
       if (p.has_post) {
-        mul_lazy<P_r>(v, x[r], p.post.w);
+        mul_r29<P_r>(v, x[r], p.post.w);
         reduce_once<P_r>(v, v);
       } else {
         reduce_once<P_r>(v, x[r]);
@@ -254,8 +257,9 @@ __global__ void ntt_tiny_kernel(fe* a, uint32_t log_n, fe w, const fe* pre_lo, c
       uint32_t c0[8], c1[8];
       ld_fe_nc(c0, pre_lo + (i & ((1u << pre_shift) - 1)));
       ld_fe_nc(c1, pre_hi + (i >> pre_shift));
-      mul<P_r>(c0, c0, c1);
-      mul<P_r>(in[i], in[i], c0);
+      mul_r29<P_r>(c0, c0, c1);
+      mul_r29<P_r>(in[i], in[i], c0);
+      reduce_once<P_r>(in[i], in[i]);
     }
   }
   uint32_t acc[8];
@@ -270,7 +274,10 @@ __global__ void ntt_tiny_kernel(fe* a, uint32_t log_n, fe w, const fe* pre_lo, c
       add<P_r>(acc, acc, t);
       mul<P_r>(wik, wik, wk);
     }
-    if (has_post) mul<P_r>(acc, acc, post.w);
+    if (has_post) {
+      mul_r29<P_r>(acc, acc, post.w);
+      reduce_once<P_r>(acc, acc);
+    }
   }
   __syncthreads();
   if (k < n) st_fe(a + k, acc);
@@ -281,7 +288,7 @@ __global__ void pow_seq_kernel(fe* out, fe base, uint64_t count, uint64_t step) 
   const uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (e >= count) return;
   uint32_t r[8];
-  pow_u64<P_r>(r, base.w, e * step);
+  pow_u64_r29<P_r>(r, base.w, e * step);
   st_fe(out + e, r);
 }
 
@@ -294,7 +301,8 @@ __global__ void twist_table_kernel(fe* out, const fe* lo, const fe* hi, uint32_t
   uint32_t a[8], b[8];
   ld_fe_nc(a, lo + (e & ((1ull << shift) - 1)));
   ld_fe_nc(b, hi + (e >> shift));
-  mul<P_r>(a, a, b);
+  mul_r29<P_r>(a, a, b);
+  reduce_once<P_r>(a, a);
   st_fe(out + idx, a);
 }
 
@@ -309,8 +317,9 @@ __global__ void scale_copy_kernel(fe* dst, const fe* src, uint64_t n, uint64_t d
     uint32_t a[8], b[8];
     ld_fe_nc(a, lo + (i & ((1ull << shift) - 1)));
     ld_fe_nc(b, hi + (i >> shift));
-    mul_lazy<P_r>(a, a, b);
-    mul<P_r>(v, v, a);
+    mul_r29<P_r>(a, a, b);
+    mul_r29<P_r>(v, v, a);
+    reduce_once<P_r>(v, v);
   }
   st_fe(dst + i * dst_stride, v);
 }
@@ -323,6 +332,9 @@ static fe to_fe(const host::Fr& a) {
   std::memcpy(r.w, a.v, 32);
   return r;
 }
+// R-form (x 2^256) -> R'-form (x 2^261): every constant the kernels multiply
+// data by (roots, twists, coset powers, scales) is kept in R' form for mul_r29.
+static fe to_fe_rp(const host::Fr& a) { return to_fe(host::mul(a, host::from_u64(32))); }
 
 static cudaError_t pow_two_level(fe** lo, fe** hi, uint32_t* shift, const host::Fr& base, int log_count,
                                  cudaStream_t s, bool pooled) {
@@ -341,8 +353,8 @@ static cudaError_t pow_two_level(fe** lo, fe** hi, uint32_t* shift, const host::
     if (e != cudaSuccess) return e;
   }
   const host::Fr bstep = host::pow_2k(base, sh);
-  pow_seq_kernel<<<(unsigned)((nlo + 255) / 256), 256, 0, s>>>(*lo, to_fe(base), nlo, 1);
-  pow_seq_kernel<<<(unsigned)((nhi + 255) / 256), 256, 0, s>>>(*hi, to_fe(bstep), nhi, 1);
+  pow_seq_kernel<<<(unsigned)((nlo + 255) / 256), 256, 0, s>>>(*lo, to_fe_rp(base), nlo, 1);
+  pow_seq_kernel<<<(unsigned)((nhi + 255) / 256), 256, 0, s>>>(*hi, to_fe_rp(bstep), nhi, 1);
   *shift = sh;
   return cudaGetLastError();
 }
@@ -383,7 +395,7 @@ static cudaError_t build_tables(NttTables* t, cudaStream_t s) {
     e = cudaMalloc((void**)&t->inner[k], half * sizeof(fe));
     if (e != cudaSuccess) return e;
     t->bytes += half * sizeof(fe);
-    pow_seq_kernel<<<(unsigned)((half + 255) / 256), 256, 0, s>>>(t->inner[k], to_fe(wm), half, 1);
+    pow_seq_kernel<<<(unsigned)((half + 255) / 256), 256, 0, s>>>(t->inner[k], to_fe_rp(wm), half, 1);
     if (k + 1 < p.npass) {
       const uint64_t total = 1ull << (b + log_J);
       e = cudaMalloc((void**)&t->twist[k], total * sizeof(fe));
@@ -438,7 +450,7 @@ cudaError_t ntt_tables_fill(NttTables* t, const host::Fr& omega, int log_n, fe* 
     const uint64_t half = b >= 1 ? (1ull << (b - 1)) : 1;
     t->inner[k] = cur;
     cur += half;
-    pow_seq_kernel<<<(unsigned)((half + 255) / 256), 256, 0, s>>>(t->inner[k], to_fe(wm), half, 1);
+    pow_seq_kernel<<<(unsigned)((half + 255) / 256), 256, 0, s>>>(t->inner[k], to_fe_rp(wm), half, 1);
     if (k + 1 < p.npass) {
       const int lc = b + log_J;
       const uint32_t sh = (uint32_t)((lc + 1) / 2);
@@ -447,8 +459,8 @@ cudaError_t ntt_tables_fill(NttTables* t, const host::Fr& omega, int log_n, fe* 
       fe* hi = cur + nlo;
       t->twist[k] = cur + nlo + nhi;
       cur += nlo + nhi + total;
-      pow_seq_kernel<<<(unsigned)((nlo + 255) / 256), 256, 0, s>>>(lo, to_fe(wMJ), nlo, 1);
-      pow_seq_kernel<<<(unsigned)((nhi + 255) / 256), 256, 0, s>>>(hi, to_fe(host::pow_2k(wMJ, sh)), nhi, 1);
+      pow_seq_kernel<<<(unsigned)((nlo + 255) / 256), 256, 0, s>>>(lo, to_fe_rp(wMJ), nlo, 1);
+      pow_seq_kernel<<<(unsigned)((nhi + 255) / 256), 256, 0, s>>>(hi, to_fe_rp(host::pow_2k(wMJ, sh)), nhi, 1);
       twist_table_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(t->twist[k], lo, hi, sh, (uint32_t)log_J,
                                                                           total);
     } else {
@@ -522,7 +534,7 @@ cudaError_t ntt_run(const NttTables& t, fe* d_a, fe* d_tmp, const PowTables* pre
   const int L = p.log_n;
   if (L <= 2) {
     fe po{};
-    if (post) po = to_fe(*post);
+    if (post) po = to_fe_rp(*post);
     ntt_tiny_kernel<<<1, 32, 0, s>>>(d_a, (uint32_t)L, to_fe(t.omega), pre ? pre->lo : nullptr, pre ? pre->hi : nullptr,
                                      pre ? pre->shift : 0u, post ? 1u : 0u, po);
     return cudaGetLastError();
@@ -547,7 +559,7 @@ cudaError_t ntt_run(const NttTables& t, fe* d_a, fe* d_tmp, const PowTables* pre
     }
     if (final_pass && post) {
       pp.has_post = 1;
-      pp.post = to_fe(*post);
+      pp.post = to_fe_rp(*post);
     }
     // buffers: single pass in place; otherwise a -> tmp, tmp in place, tmp -> a
     if (p.npass == 1) {
