@@ -68,6 +68,16 @@ def test_msm_edge_cases(zk, oracle):
     assert np.array_equal(affine_of(zk.msm(s5, pts)), oracle.multiexp(s5, pts))
 
 
+@pytest.mark.parametrize("value", [1, 2**15, 2**16 + 1, 7])
+def test_msm_skewed_buckets(zk, oracle, value):
+    """every scalar equal: each window's points all land in one bucket, which
+    the sub-bucket split and the block-wide reduction must handle"""
+    n = 1 << 16
+    s = np.tile(oracle.to_mont(value), (n, 1))
+    pts, k = oracle.rand_bases(n, 40 + value % 97, with_dlog=True)
+    assert np.array_equal(affine_of(zk.msm(s, pts)), oracle.msm_by_dlog(s, k))
+
+
 def test_msm_small_scalar_mix(zk, oracle):
     n = 1 << 16
     s = oracle.rand_fr(n, 12)

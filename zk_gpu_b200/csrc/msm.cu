@@ -121,17 +121,40 @@ __global__ void scan_add_kernel(uint32_t* out, uint32_t* cursor, const uint32_t*
   cursor[i] = v;
 }
 
-// One thread per bucket: sum of its (signed) points.
-__global__ void __launch_bounds__(256) msm_bucket_kernel(const uint32_t* list, const uint32_t* offsets,
-                                                         const uint32_t* counts, const fe* bases, fe* buckets,
-                                                         uint32_t total_buckets) {
+// Buckets are split into sub-buckets of at most SUB entries, one thread
+// each, so a bucket that collects a large share of the points (skewed
+// scalars, e.g. many small ones all carrying into the same digit) is summed
+// by many threads instead of one.
+constexpr uint32_t SUB = 64;          // entries per sub-bucket
+constexpr uint32_t SEQ_MAX = 16;      // sub-sums a bucket combines in one thread
+
+__global__ void msm_nsub_kernel(const uint32_t* counts, uint32_t* nsub, uint32_t total) {
   const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= total_buckets) return;
-  const uint32_t beg = offsets[b], cnt = counts[b];
+  if (b < total) nsub[b] = (counts[b] + SUB - 1) / SUB;
+}
+
+__global__ void msm_submap_kernel(const uint32_t* nsub, const uint32_t* sub_off, uint32_t* sub2b, uint32_t total) {
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= total) return;
+  const uint32_t k = nsub[b], o = sub_off[b];
+  for (uint32_t j = 0; j < k; j++) sub2b[o + j] = b;
+}
+
+// One thread per sub-bucket: sum of its (signed) points.
+__global__ void __launch_bounds__(256) msm_subbucket_kernel(const uint32_t* list, const uint32_t* offsets,
+                                                            const uint32_t* counts, const uint32_t* sub_off,
+                                                            const uint32_t* sub2b, const uint32_t* total_sub,
+                                                            const fe* bases, fe* subres) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= *total_sub) return;
+  const uint32_t b = sub2b[s];
+  const uint32_t j = s - sub_off[b];
+  const uint32_t beg = offsets[b] + j * SUB;
+  const uint32_t end = min(offsets[b] + counts[b], beg + SUB);
   xyzz_t acc;
   xyzz_set_inf(acc);
-  for (uint32_t k = 0; k < cnt; k++) {
-    const uint32_t e = list[beg + k];
+  for (uint32_t k = beg; k < end; k++) {
+    const uint32_t e = list[k];
     aff_t q;
     ld_aff(q, bases + 2 * (uint64_t)(e & 0x7fffffffu));
     if (aff_is_inf(q)) continue;
@@ -141,7 +164,58 @@ __global__ void __launch_bounds__(256) msm_bucket_kernel(const uint32_t* list, c
     }
     xyzz_madd(acc, q);
   }
+  st_xyzz(subres + 4 * (uint64_t)s, acc);
+}
+
+// One thread per bucket: combine its sub-sums when there are few; queue the
+// bucket for the block-wide reduction when there are many.
+__global__ void msm_bucket_final_kernel(const uint32_t* nsub, const uint32_t* sub_off, const fe* subres, fe* buckets,
+                                        uint32_t* heavy, uint32_t* heavy_count, uint32_t total) {
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= total) return;
+  const uint32_t k = nsub[b], o = sub_off[b];
+  if (k > SEQ_MAX) {
+    heavy[atomicAdd(heavy_count, 1u)] = b;
+    return;
+  }
+  xyzz_t acc, t;
+  xyzz_set_inf(acc);
+  for (uint32_t j = 0; j < k; j++) {
+    ld_xyzz(t, subres + 4 * (uint64_t)(o + j));
+    xyzz_add(acc, t);
+  }
   st_xyzz(buckets + 4 * (uint64_t)b, acc);
+}
+
+// One block per queued heavy bucket: strided partial sums, then a tree.
+__global__ void __launch_bounds__(256) msm_heavy_kernel(const uint32_t* nsub, const uint32_t* sub_off,
+                                                        const fe* subres, fe* buckets, const uint32_t* heavy,
+                                                        const uint32_t* heavy_count) {
+  __shared__ fe sh[256 * 4];
+  if (blockIdx.x >= *heavy_count) return;
+  const uint32_t b = heavy[blockIdx.x];
+  const uint32_t k = nsub[b], o = sub_off[b];
+  xyzz_t acc, t;
+  xyzz_set_inf(acc);
+  for (uint32_t j = threadIdx.x; j < k; j += blockDim.x) {
+    ld_xyzz(t, subres + 4 * (uint64_t)(o + j));
+    xyzz_add(acc, t);
+  }
+  st_xyzz(sh + 4 * threadIdx.x, acc);
+  __syncthreads();
+  for (uint32_t half = blockDim.x / 2; half > 0; half >>= 1) {
+    if (threadIdx.x < half) {
+      ld_xyzz(acc, sh + 4 * threadIdx.x);
+      ld_xyzz(t, sh + 4 * (threadIdx.x + half));
+      xyzz_add(acc, t);
+      st_xyzz(sh + 4 * threadIdx.x, acc);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    ld_xyzz(acc, sh);
+    st_xyzz(buckets + 4 * (uint64_t)b, acc);
+  }
 }
 
 // Per (window, segment): running sums over the segment's buckets, top down,
@@ -231,9 +305,14 @@ cudaError_t msm_run(const fe* d_scalars, const fe* d_bases, uint64_t n, fe* d_ou
   const uint32_t total = W * B;
   const uint32_t nblk = (total + 1023) / 1024;
   const uint64_t entries = n * (uint64_t)W;
+  if (entries >= (1ull << 32)) return cudaErrorInvalidValue;  // entry offsets are 32-bit
   uint32_t *counts = nullptr, *offsets = nullptr, *cursor = nullptr, *bsums = nullptr, *list = nullptr;
-  fe *buckets = nullptr, *segres = nullptr, *winsum = nullptr;
+  uint32_t *nsub = nullptr, *sub_off = nullptr, *sub2b = nullptr, *heavy = nullptr, *heavy_count = nullptr;
+  fe *buckets = nullptr, *segres = nullptr, *winsum = nullptr, *subres = nullptr;
   const uint32_t segs = total / L;
+  // sum_b ceil(count_b / SUB) <= entries / SUB + total; heavy buckets have > SEQ_MAX * SUB entries
+  const uint64_t max_sub = entries / SUB + total + 1;
+  const uint64_t max_heavy = entries / ((uint64_t)SEQ_MAX * SUB) + 1;
   cudaError_t e = cudaSuccess;
   auto alloc = [&](void** ptr, size_t bytes) {
     if (e == cudaSuccess) e = cudaMallocAsync(ptr, bytes, s);
@@ -243,13 +322,21 @@ cudaError_t msm_run(const fe* d_scalars, const fe* d_bases, uint64_t n, fe* d_ou
   alloc((void**)&cursor, total * 4ull);
   alloc((void**)&bsums, (nblk + 1) * 4ull);
   alloc((void**)&list, entries * 4ull);
+  alloc((void**)&nsub, total * 4ull);
+  alloc((void**)&sub_off, (total + 1) * 4ull);
+  alloc((void**)&sub2b, max_sub * 4ull);
+  alloc((void**)&heavy, max_heavy * 4ull);
+  alloc((void**)&heavy_count, 4ull);
+  alloc((void**)&subres, max_sub * 128ull);
   alloc((void**)&buckets, total * 128ull);
   alloc((void**)&segres, segs * 128ull);
   alloc((void**)&winsum, W * 128ull);
   if (e == cudaSuccess) {
     const double nd = (double)n;
     cudaMemsetAsync(counts, 0, total * 4ull, s);
+    cudaMemsetAsync(heavy_count, 0, 4ull, s);
     const unsigned g = (unsigned)((n + 255) / 256);
+    const unsigned gb = (total + 255) / 256;
     {
       ProfScope ps("msm_count", s, nd, nd * 32);
       msm_count_kernel<<<g, 256, 0, s>>>(d_scalars, n, (uint32_t)p.c, W, counts);
@@ -261,10 +348,21 @@ cudaError_t msm_run(const fe* d_scalars, const fe* d_bases, uint64_t n, fe* d_ou
       ProfScope ps("msm_scatter", s, nd, nd * 32 + (double)entries * 4);
       msm_scatter_kernel<<<g, 256, 0, s>>>(d_scalars, n, (uint32_t)p.c, W, cursor, list);
     }
+    msm_nsub_kernel<<<gb, 256, 0, s>>>(counts, nsub, total);
+    scan_block_kernel<<<nblk, 1024, 0, s>>>(nsub, sub_off, bsums, total);
+    scan_sums_kernel<<<1, 1024, 0, s>>>(bsums, nblk, sub_off + total);
+    scan_add_kernel<<<nblk, 1024, 0, s>>>(sub_off, cursor, bsums, total);
+    msm_submap_kernel<<<gb, 256, 0, s>>>(nsub, sub_off, sub2b, total);
     {
       // convention: 6 Fq products per point-window (batch-affine cost)
-      ProfScope ps("msm_bucket", s, (double)entries * 6, (double)entries * (64 + 4) + total * 128.0);
-      msm_bucket_kernel<<<(total + 255) / 256, 256, 0, s>>>(list, offsets, counts, d_bases, buckets, total);
+      ProfScope ps("msm_bucket", s, (double)entries * 6, (double)entries * (64 + 4) + max_sub * 128.0);
+      msm_subbucket_kernel<<<(unsigned)((max_sub + 255) / 256), 256, 0, s>>>(list, offsets, counts, sub_off, sub2b,
+                                                                              sub_off + total, d_bases, subres);
+    }
+    {
+      ProfScope ps("msm_bucket_final", s, (double)total * 14, total * 256.0);
+      msm_bucket_final_kernel<<<gb, 256, 0, s>>>(nsub, sub_off, subres, buckets, heavy, heavy_count, total);
+      msm_heavy_kernel<<<(unsigned)max_heavy, 256, 0, s>>>(nsub, sub_off, subres, buckets, heavy, heavy_count);
     }
     {
       ProfScope ps("msm_segment", s, (double)total * 2 * 14, total * 128.0);
@@ -272,17 +370,13 @@ cudaError_t msm_run(const fe* d_scalars, const fe* d_bases, uint64_t n, fe* d_ou
     }
     msm_window_kernel<<<W, 256, 0, s>>>(segres, winsum, B / L);
     msm_combine_kernel<<<1, 32, 0, s>>>(winsum, W, (uint32_t)p.c, d_out);
-    nl = 9;
+    nl = 16;
     e = cudaGetLastError();
   }
-  if (counts) cudaFreeAsync(counts, s);
-  if (offsets) cudaFreeAsync(offsets, s);
-  if (cursor) cudaFreeAsync(cursor, s);
-  if (bsums) cudaFreeAsync(bsums, s);
-  if (list) cudaFreeAsync(list, s);
-  if (buckets) cudaFreeAsync(buckets, s);
-  if (segres) cudaFreeAsync(segres, s);
-  if (winsum) cudaFreeAsync(winsum, s);
+  for (void* ptr : {(void*)counts, (void*)offsets, (void*)cursor, (void*)bsums, (void*)list, (void*)nsub,
+                    (void*)sub_off, (void*)sub2b, (void*)heavy, (void*)heavy_count, (void*)subres, (void*)buckets,
+                    (void*)segres, (void*)winsum})
+    if (ptr) cudaFreeAsync(ptr, s);
   if (launches) *launches = nl;
   return e;
 }
