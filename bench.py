@@ -300,6 +300,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     msm_ms = max_over_ranks(e0.elapsed_time(e1) / msm_steps)
     del d_sc, d_bs
 
+    batched = bench_batched(zk, torch, dev, stream, args.steps)
+
     # ---- e2e through the host-buffer C ABI, pinned host memory ----
     h_vals = torch.from_numpy(vals_np.view(np.int64)).pin_memory()
     h_ext = torch.empty((N, 4), dtype=torch.int64).pin_memory()
@@ -353,7 +355,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                   "msm_2p22_mpts_s": round(world * n_msm / (msm_ms * 1e-3) / 1e6, 2),
                   "msm_2p22_ms": round(msm_ms, 3),
                   "msm_kernels": {k: {"launches": v["launches"], "ms": round(v["ms"], 3)} for k, v in msm_prof.items()},
-                  "msm_roofline": msm_roofline(msm_prof, imad_ps, n_msm, msm_ms)},
+                  "msm_roofline": msm_roofline(msm_prof, imad_ps, n_msm, msm_ms),
+                  "batched_ntt": batched},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         t, threads = cpu_lde_sample()
@@ -367,6 +370,77 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def bench_batched(zk, torch, dev: int, stream, steps: int, njobs: int = 512, seed: int = 77):
+    """512 NTT jobs, log2 size uniform in {10..20}, random forward/inverse and
+    coset flag: one persistent graph launch per run vs one call per job."""
+    rng = np.random.default_rng(seed)
+    sizes = [int(k) for k in rng.integers(10, 21, njobs)]
+    gen = torch.Generator(device=f"cuda:{dev}")
+    gen.manual_seed(seed)
+    consts = {}
+    jobs = []
+    for k in sizes:
+        if k not in consts:
+            w = root_of_unity(k)
+            consts[k] = (mont(w), mont(pow(w, -1, R_MOD)), mont(pow(1 << k, -1, R_MOD)),
+                         mont(7 * root_of_unity(k + 2) % R_MOD))
+        w, wi, ninv, c = consts[k]
+        # uniform 252-bit values (< r), generated on the device
+        t = torch.randint(0, 2**62, (1 << k, 4), dtype=torch.int64, device=f"cuda:{dev}", generator=gen)
+        t[:, 3] &= (1 << 60) - 1
+        inverse, coset = bool(rng.integers(0, 2)), bool(rng.integers(0, 2))
+        j = {"tensor": t, "log_n": k, "omega": wi if inverse else w}
+        if inverse:
+            j["scale"] = ninv
+        if coset:
+            j["coset"] = c
+        jobs.append(j)
+    elems = sum(1 << k for k in sizes)
+    batch = zk.NttBatch(jobs, device=dev)
+    for _ in range(2):
+        batch.run(stream)
+    stream.synchronize()
+    batch.check()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    runs = max(3, min(steps, 10))
+    zk.launch_count(reset=True)
+    e0.record(stream)
+    for _ in range(runs):
+        batch.run(stream)
+    e1.record(stream)
+    stream.synchronize()
+    batch_launches = zk.launch_count() / runs
+    batch.check()
+    batch_ms = e0.elapsed_time(e1) / runs
+
+    def one_call_per_job():
+        for j in jobs:
+            zk.ntt_dev(j["tensor"], j["log_n"], j["omega"], coset=j.get("coset"), post_scale=j.get("scale"),
+                       stream=stream)
+
+    one_call_per_job()
+    stream.synchronize()
+    zk.launch_count(reset=True)
+    e0.record(stream)
+    for _ in range(runs):
+        one_call_per_job()
+    e1.record(stream)
+    stream.synchronize()
+    single_launches = zk.launch_count() / runs
+    single_ms = e0.elapsed_time(e1) / runs
+    info = batch.info()
+    batch.close()
+    return {"jobs": njobs, "elements": elems, "batched_ms": round(batch_ms, 3),
+            "batched_jobs_s": round(njobs / (batch_ms * 1e-3), 1),
+            "batched_melem_s": round(elems / (batch_ms * 1e-3) / 1e6, 1),
+            "one_call_per_job_ms": round(single_ms, 3),
+            "one_call_per_job_jobs_s": round(njobs / (single_ms * 1e-3), 1),
+            "speedup": round(single_ms / batch_ms, 3),
+            "launches_per_run": {"batched": batch_launches, "one_call_per_job": single_launches},
+            "work_items": info["tiles"], "passes": info["passes"], "grid": info["grid"],
+            "inputs": "uniform 252-bit values (< r) from torch.randint on the device"}
 
 
 def small_fr(n: int, seed: int, bits: int = 16) -> np.ndarray:

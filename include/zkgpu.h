@@ -132,6 +132,31 @@ int zkgpu_msm_dev(int device, const uint64_t *d_scalars, const uint64_t *d_bases
                   void *stream);
 
 /* ======================================================================
+ * Batched NTTs: many transforms of uneven sizes in one persistent launch,
+ * replayed from a CUDA graph.  Replaces the per-job device choice and
+ * one-call-per-job flow of src/gpulock.rs:133-226 + cuda/fft.cu:275-405.
+ * ====================================================================== */
+#define ZKGPU_JOB_COSET 1u /* multiply element i by coset^i before the transform */
+#define ZKGPU_JOB_SCALE 2u /* multiply every output by scale (e.g. n^-1 for an inverse) */
+typedef struct {
+    uint64_t *data;     /* device memory, 2^log_n elements, transformed in place */
+    uint32_t log_n;     /* 3 .. 28 */
+    uint32_t flags;     /* ZKGPU_JOB_* */
+    uint64_t omega[4];  /* root of order exactly 2^log_n (w^-1 for an inverse) */
+    uint64_t coset[4];
+    uint64_t scale[4];
+} zkgpu_ntt_job;
+/* Build a batch (tables, scratch, work list, graph).  The jobs' data
+ * pointers are baked in: refill the same buffers and run again. */
+int zkgpu_ntt_batch_create(int device, const zkgpu_ntt_job *jobs, uint32_t njobs, void **handle);
+/* Enqueue one run on `stream` (graph launch); one run at a time per handle. */
+int zkgpu_ntt_batch_run(void *handle, void *stream);
+/* After a run completed: ZKGPU_ETIMEOUT if a bounded dependency wait expired. */
+int zkgpu_ntt_batch_check(void *handle);
+void zkgpu_ntt_batch_info(void *handle, uint32_t *passes, uint32_t *tiles, int *grid);
+void zkgpu_ntt_batch_destroy(void *handle);
+
+/* ======================================================================
  * Diagnostics.
  * ====================================================================== */
 /* elementwise field op on host arrays through the device kernels:

@@ -66,6 +66,11 @@ EXPORTS = {
     "zkgpu_lagrange_to_extended_dev": (_i32, [_i32, P, _u32, P, _u32, P, P, P, P, P]),
     "zkgpu_msm_dev": (_i32, [_i32, P, P, _u64, P, P]),
     "zkgpu_ntt_dev_static": (_i32, [_i32, P, _u32, P, P]),
+    "zkgpu_ntt_batch_create": (_i32, [_i32, P, _u32, P]),
+    "zkgpu_ntt_batch_run": (_i32, [P, P]),
+    "zkgpu_ntt_batch_check": (_i32, [P]),
+    "zkgpu_ntt_batch_info": (None, [P, P, P, P]),
+    "zkgpu_ntt_batch_destroy": (None, [P]),
     "zkgpu_field_op": (_i32, [_i32, _i32, _i32, P, P, P, _u64]),
     "zkgpu_last_error": (ctypes.c_char_p, []),
     "zkgpu_launch_count": (_u64, [_i32]),
@@ -251,6 +256,61 @@ def lagrange_to_extended_dev(values, ext, log_n: int, log_ext: int, omega_inv, d
     _check(lib().zkgpu_lagrange_to_extended_dev(dev, _ptr(values), log_n, _ptr(ext), log_ext, wi.ctypes.data,
                                                 d.ctypes.data, gg.ctypes.data, we.ctypes.data, _stream_ptr(stream)),
            "lagrange_to_extended_dev")
+
+
+JOB_COSET, JOB_SCALE = 1, 2
+
+
+class NttJob(ctypes.Structure):
+    """zkgpu_ntt_job (include/zkgpu.h)"""
+    _fields_ = [("data", ctypes.c_void_p), ("log_n", ctypes.c_uint32), ("flags", ctypes.c_uint32),
+                ("omega", ctypes.c_uint64 * 4), ("coset", ctypes.c_uint64 * 4), ("scale", ctypes.c_uint64 * 4)]
+
+
+class NttBatch:
+    """Many in-place NTTs of uneven sizes run by one persistent launch from a
+    captured CUDA graph.  jobs: dicts with keys tensor (CUDA, (2^log_n, 4)),
+    log_n, omega, and optional coset, scale."""
+
+    def __init__(self, jobs: list, device: int = 0):
+        arr = (NttJob * len(jobs))()
+        for i, j in enumerate(jobs):
+            arr[i].data = _ptr(j["tensor"])
+            arr[i].log_n = j["log_n"]
+            flags = 0
+            arr[i].omega[:] = [int(v) for v in _el(j["omega"])]
+            if j.get("coset") is not None:
+                flags |= JOB_COSET
+                arr[i].coset[:] = [int(v) for v in _el(j["coset"])]
+            if j.get("scale") is not None:
+                flags |= JOB_SCALE
+                arr[i].scale[:] = [int(v) for v in _el(j["scale"])]
+            arr[i].flags = flags
+        self._jobs = arr
+        self.handle = ctypes.c_void_p()
+        _check(lib().zkgpu_ntt_batch_create(device, arr, len(jobs), ctypes.byref(self.handle)), "ntt_batch_create")
+
+    def run(self, stream=None):
+        _check(lib().zkgpu_ntt_batch_run(self.handle, _stream_ptr(stream)), "ntt_batch_run")
+
+    def check(self):
+        _check(lib().zkgpu_ntt_batch_check(self.handle), "ntt_batch_check")
+
+    def info(self) -> dict:
+        p, t, g = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_int()
+        lib().zkgpu_ntt_batch_info(self.handle, ctypes.byref(p), ctypes.byref(t), ctypes.byref(g))
+        return {"passes": p.value, "tiles": t.value, "grid": g.value}
+
+    def close(self):
+        if self.handle:
+            lib().zkgpu_ntt_batch_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def msm_dev(scalars, bases, out, stream=None):

@@ -1,0 +1,210 @@
+// batch.cu — many NTTs of uneven sizes in ONE persistent launch, replayed
+// from a captured CUDA graph.
+//
+// This is the single-GPU replacement of the reference's job scheduling
+// (src/gpulock.rs:133-226 picks a device and the caller then makes one
+// synchronous FFI call per job, each with its own malloc / H2D / five
+// launches / D2H, cuda/fft.cu:275-405).  Here a batch is built once from job
+// descriptors (device-resident data), every pass of every job becomes a run
+// of CTA tiles in one level-ordered work list, and a persistent kernel
+// (ntt_batch_kernel) drains the list; a graph holding {counter reset, kernel}
+// is replayed for each run.
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
+#include "ntt.cuh"
+#include "runtime.cuh"
+
+namespace zk {
+
+namespace {
+struct PowKey {
+  int dev, log_n;
+  uint64_t c[4];
+  bool operator<(const PowKey& o) const {
+    return std::tie(dev, log_n, c[0], c[1], c[2], c[3]) < std::tie(o.dev, o.log_n, o.c[0], o.c[1], o.c[2], o.c[3]);
+  }
+};
+std::mutex g_pow_mu;
+std::map<PowKey, PowTables> g_pow_cache;
+}  // namespace
+
+// Coset power tables cached per (device, c, log_n): batches and the serving
+// loop reuse the same few cosets (the field generator and its shifts).
+const PowTables* pow_tables_get(int device, const host::Fr& c, int log_n, cudaStream_t s, cudaError_t* err) {
+  PowKey k{device, log_n, {c.v[0], c.v[1], c.v[2], c.v[3]}};
+  std::lock_guard<std::mutex> lk(g_pow_mu);
+  auto it = g_pow_cache.find(k);
+  if (it != g_pow_cache.end()) {
+    *err = cudaSuccess;
+    return &it->second;
+  }
+  PowTables t;
+  cudaError_t e = pow_tables_make(&t, c, log_n, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  *err = e;
+  if (e != cudaSuccess) return nullptr;
+  return &g_pow_cache.emplace(k, t).first->second;
+}
+
+struct NttBatch {
+  int device = 0;
+  BatchPass* d_passes = nullptr;
+  uint32_t npass = 0, total_tiles = 0;
+  uint32_t* d_counters = nullptr;  // [0] next, [1] err, [2..] done per pass
+  fe* d_tmp = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int grid = 0;
+  uint64_t launches_per_run = 2;
+  ~NttBatch() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (d_passes) cudaFree(d_passes);
+    if (d_counters) cudaFree(d_counters);
+    if (d_tmp) cudaFree(d_tmp);
+  }
+};
+
+}  // namespace zk
+
+using zk::fe;
+namespace hf = zk::host;
+
+static hf::Fr fr_of(const uint64_t v[4]) {
+  hf::Fr r;
+  std::memcpy(r.v, v, 32);
+  return r;
+}
+
+extern "C" int zkgpu_ntt_batch_create(int device, const zkgpu_ntt_job* jobs, uint32_t njobs, void** out) {
+  if (!out || (njobs && !jobs)) return ZKGPU_EINVAL;
+  *out = nullptr;
+  cudaStream_t s;
+  int st = zk::bind_device(device, &s);
+  if (st) return st;
+  auto b = std::make_unique<zk::NttBatch>();
+  b->device = device;
+  // validate and collect per-job tables
+  struct JobInfo {
+    const zk::NttTables* t;
+    const zk::PowTables* pre;
+    hf::Fr post;
+    bool has_post;
+    size_t tmp_off;
+  };
+  std::vector<JobInfo> info(njobs);
+  size_t tmp_elems = 0;
+  int max_pass = 0;
+  for (uint32_t j = 0; j < njobs; j++) {
+    const zkgpu_ntt_job& jb = jobs[j];
+    if (!jb.data || jb.log_n < 3 || jb.log_n > (uint32_t)zk::NTT_MAX_LOG) return ZKGPU_EINVAL;
+    hf::Fr w = fr_of(jb.omega);
+    if (!hf::is_canonical(w) || !hf::is_primitive_root(w, jb.log_n)) return ZKGPU_EINVAL;
+    cudaError_t e;
+    info[j].t = zk::ntt_tables_get(device, w, (int)jb.log_n, s, &e);
+    if (!info[j].t) return zk::status_of("ntt_tables_get", e);
+    info[j].pre = nullptr;
+    if (jb.flags & ZKGPU_JOB_COSET) {
+      hf::Fr c = fr_of(jb.coset);
+      if (!hf::is_canonical(c)) return ZKGPU_EINVAL;
+      info[j].pre = zk::pow_tables_get(device, c, (int)jb.log_n, s, &e);
+      if (!info[j].pre) return zk::status_of("pow_tables_get", e);
+    }
+    info[j].has_post = (jb.flags & ZKGPU_JOB_SCALE) != 0;
+    if (info[j].has_post) {
+      info[j].post = fr_of(jb.scale);
+      if (!hf::is_canonical(info[j].post)) return ZKGPU_EINVAL;
+    }
+    info[j].tmp_off = tmp_elems;
+    if (info[j].t->plan.npass > 1) tmp_elems += (size_t)1 << jb.log_n;
+    if (info[j].t->plan.npass > max_pass) max_pass = info[j].t->plan.npass;
+  }
+  if (tmp_elems) ZK_TRY("cudaMalloc(batch scratch)", cudaMalloc((void**)&b->d_tmp, tmp_elems * sizeof(fe)));
+  // level-ordered pass list
+  std::vector<zk::BatchPass> passes;
+  std::vector<uint32_t> prev_index(njobs, ~0u);
+  uint64_t tiles = 0;
+  for (int lvl = 0; lvl < max_pass; lvl++) {
+    for (uint32_t j = 0; j < njobs; j++) {
+      const zk::NttTables& t = *info[j].t;
+      if (lvl >= t.plan.npass) continue;
+      zk::BatchPass bp{};
+      const uint64_t ncta = zk::ntt_pass_params(t, lvl, reinterpret_cast<fe*>(jobs[j].data), b->d_tmp + info[j].tmp_off,
+                                                info[j].pre, info[j].has_post ? &info[j].post : nullptr, &bp.p);
+      bp.B = (uint32_t)t.plan.bits[lvl];
+      bp.ntiles = (uint32_t)ncta;
+      bp.tile_base = (uint32_t)tiles;
+      bp.dep = prev_index[j];
+      bp.dep_tiles = bp.dep == ~0u ? 0u : passes[bp.dep].ntiles;
+      prev_index[j] = (uint32_t)passes.size();
+      passes.push_back(bp);
+      tiles += ncta;
+    }
+  }
+  if (tiles >= (1ull << 32)) return ZKGPU_EINVAL;
+  b->npass = (uint32_t)passes.size();
+  b->total_tiles = (uint32_t)tiles;
+  if (b->npass) {
+    ZK_TRY("cudaMalloc(batch passes)", cudaMalloc((void**)&b->d_passes, passes.size() * sizeof(zk::BatchPass)));
+    ZK_TRY("batch passes H2D", cudaMemcpy(b->d_passes, passes.data(), passes.size() * sizeof(zk::BatchPass),
+                                          cudaMemcpyHostToDevice));
+  }
+  ZK_TRY("cudaMalloc(batch counters)", cudaMalloc((void**)&b->d_counters, (2 + b->npass) * sizeof(uint32_t)));
+  ZK_TRY("cudaMemset", cudaMemset(b->d_counters, 0, (2 + b->npass) * sizeof(uint32_t)));
+  b->grid = zk::ntt_batch_grid(device);
+  // capture {reset counters, persistent kernel} once
+  cudaStream_t cap;
+  ZK_TRY("cudaStreamCreate", cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+  cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    cudaMemsetAsync(b->d_counters, 0, (2 + b->npass) * sizeof(uint32_t), cap);
+    if (b->npass)
+      zk::ntt_batch_launch(b->d_passes, b->npass, b->total_tiles, b->d_counters, b->d_counters + 2,
+                           b->d_counters + 1, b->grid, cap);
+    e = cudaStreamEndCapture(cap, &b->graph);
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, b->graph, 0);
+  cudaStreamDestroy(cap);
+  if (e != cudaSuccess) return zk::status_of("batch graph", e);
+  *out = b.release();
+  return ZKGPU_OK;
+}
+
+extern "C" int zkgpu_ntt_batch_run(void* handle, void* stream) {
+  auto* b = static_cast<zk::NttBatch*>(handle);
+  if (!b) return ZKGPU_EINVAL;
+  ZK_TRY("cudaSetDevice", cudaSetDevice(b->device));
+  ZK_TRY("cudaGraphLaunch", cudaGraphLaunch(b->exec, (cudaStream_t)stream));
+  zk::count_launches(b->npass ? 1 : 0);
+  return ZKGPU_OK;
+}
+
+extern "C" int zkgpu_ntt_batch_check(void* handle) {
+  auto* b = static_cast<zk::NttBatch*>(handle);
+  if (!b) return ZKGPU_EINVAL;
+  ZK_TRY("cudaSetDevice", cudaSetDevice(b->device));
+  uint32_t err = 0;
+  ZK_TRY("batch err D2H", cudaMemcpy(&err, b->d_counters + 1, 4, cudaMemcpyDeviceToHost));
+  return err ? ZKGPU_ETIMEOUT : ZKGPU_OK;
+}
+
+extern "C" void zkgpu_ntt_batch_info(void* handle, uint32_t* passes, uint32_t* tiles, int* grid) {
+  auto* b = static_cast<zk::NttBatch*>(handle);
+  if (!b) return;
+  if (passes) *passes = b->npass;
+  if (tiles) *tiles = b->total_tiles;
+  if (grid) *grid = b->grid;
+}
+
+extern "C" void zkgpu_ntt_batch_destroy(void* handle) {
+  auto* b = static_cast<zk::NttBatch*>(handle);
+  if (!b) return;
+  cudaSetDevice(b->device);
+  cudaDeviceSynchronize();
+  delete b;
+}

@@ -449,6 +449,13 @@ __device__ __forceinline__ void ld_fe_nc(uint32_t r[8], const fe* p) {
   r[0] = x.x; r[1] = x.y; r[2] = x.z; r[3] = x.w;
   r[4] = y.x; r[5] = y.y; r[6] = y.z; r[7] = y.w;
 }
+// through L2 only: data another CTA of the same launch may have written
+__device__ __forceinline__ void ld_fe_cg(uint32_t r[8], const fe* p) {
+  const uint4* q = reinterpret_cast<const uint4*>(p);
+  uint4 x = __ldcg(q), y = __ldcg(q + 1);
+  r[0] = x.x; r[1] = x.y; r[2] = x.z; r[3] = x.w;
+  r[4] = y.x; r[5] = y.y; r[6] = y.z; r[7] = y.w;
+}
 __device__ __forceinline__ void st_fe(fe* p, const uint32_t r[8]) {
   uint4* q = reinterpret_cast<uint4*>(p);
   q[0] = make_uint4(r[0], r[1], r[2], r[3]);

@@ -34,7 +34,7 @@ NttPlan make_ntt_plan(int log_n) {
     p.npass = 0;
     return p;
   }
-  if (log_n <= 12) {
+  if (log_n <= 11) {
     p.npass = 1;
     p.bits[0] = log_n;
     return p;
@@ -104,60 +104,51 @@ __device__ __forceinline__ void ntt_round(uint32_t x[8][8], uint32_t q, const ui
 
 template <int B, int LO_CUR, int LO_NEXT>
 __device__ __forceinline__ void ntt_exchange(uint32_t x[8][8], uint32_t q, uint32_t gbase, uint32_t* sm,
-                                             uint32_t plane_stride) {
+                                             uint32_t plane_stride, bool active) {
+  if (active) {
 #pragma unroll
-  for (int r = 0; r < 8; r++) st_smem_fe(sm, plane_stride, swz(gbase + ins3<LO_CUR>(q, r)), x[r]);
+    for (int r = 0; r < 8; r++) st_smem_fe(sm, plane_stride, swz(gbase + ins3<LO_CUR>(q, r)), x[r]);
+  }
   __syncthreads();
+  if (active) {
 #pragma unroll
-  for (int r = 0; r < 8; r++) ld_smem_fe(x[r], sm, plane_stride, swz(gbase + ins3<LO_NEXT>(q, r)));
+    for (int r = 0; r < 8; r++) ld_smem_fe(x[r], sm, plane_stride, swz(gbase + ins3<LO_NEXT>(q, r)));
+  }
   __syncthreads();
 }
 
 template <int B, int HI>
 __device__ __forceinline__ void ntt_rounds(uint32_t x[8][8], uint32_t q, uint32_t gbase, uint32_t* sm,
-                                           uint32_t plane_stride, const uint32_t* tws) {
+                                           uint32_t plane_stride, const uint32_t* tws, bool active) {
   constexpr int LO = HI - 3 > 0 ? HI - 3 : 0;
   ntt_round<B, LO, HI>(x, q, tws);
   if constexpr (LO > 0) {
     constexpr int LO_N = LO - 3 > 0 ? LO - 3 : 0;
-    ntt_exchange<B, LO, LO_N>(x, q, gbase, sm, plane_stride);
-    ntt_rounds<B, LO>(x, q, gbase, sm, plane_stride, tws);
+    ntt_exchange<B, LO, LO_N>(x, q, gbase, sm, plane_stride, active);
+    ntt_rounds<B, LO>(x, q, gbase, sm, plane_stride, tws, active);
   }
 }
 
-struct PassParams {
-  const fe* in;
-  fe* out;
-  const fe* inner;   // w_m^e, e < m/2
-  const fe* twist;   // [k * J + j], non-final passes
-  const fe* pre_lo;  // coset powers (first pass), or null
-  const fe* pre_hi;
-  uint32_t pre_shift;
-  uint32_t log_J;
-  uint32_t log_O;
-  uint32_t log_m1;
-  uint32_t nprev;
-  uint32_t prev_bits[NTT_MAX_PASS];
-  uint32_t G;
-  uint32_t is_final;
-  uint32_t has_post;
-  fe post;
-};
 
 #ifndef ZK_NTT_MIN_BLOCKS
 #define ZK_NTT_MIN_BLOCKS 2
 #endif
-template <int B>
-__global__ void __launch_bounds__(B >= 12 ? 512 : 256, B >= 12 ? 1 : ZK_NTT_MIN_BLOCKS) ntt_pass_kernel(const PassParams p) {
+
+// One CTA tile of one pass.  `tile` plays the role of the block index.  In
+// BATCH mode the CTA may be wider than the tile (G * T threads are active,
+// the rest only join the barriers) and data is read through L2 only, since
+// other CTAs of the same launch produced it.
+template <int B, bool BATCH>
+__device__ __forceinline__ void ntt_pass_tile(const PassParams& p, uint64_t tile, uint32_t* smem) {
   constexpr uint32_t M = 1u << B;
   constexpr uint32_t T = M / 8;  // threads per column
-  extern __shared__ uint32_t smem[];
   const uint32_t G = p.G;
   const uint32_t plane_stride = G * M;
   uint32_t* tws = smem + 8 * plane_stride;
 
   const uint32_t tid = threadIdx.x;
   const uint32_t g = tid / T, q = tid % T;
+  const bool active = !BATCH || g < G;
 
   for (uint32_t e = tid; e < M / 2; e += blockDim.x) {
     uint32_t w[8];
@@ -169,24 +160,34 @@ __global__ void __launch_bounds__(B >= 12 ? 512 : 256, B >= 12 ? 1 : ZK_NTT_MIN_
   uint64_t o, col = 0, base, stride;
   if (!p.is_final) {
     const uint64_t cols_per_o = J / G;
-    o = blockIdx.x / cols_per_o;
-    col = (blockIdx.x % cols_per_o) * G + g;
+    o = tile / cols_per_o;
+    col = (tile % cols_per_o) * G + g;
     base = o * (uint64_t)M * J + col;
     stride = J;
   } else {
     const uint64_t rest_count = (1ull << p.log_O) >> p.log_m1;
-    const uint64_t rest = blockIdx.x % rest_count;
-    const uint64_t k1 = (blockIdx.x / rest_count) * G + g;
+    const uint64_t rest = tile % rest_count;
+    const uint64_t k1 = (tile / rest_count) * G + g;
     o = k1 * rest_count + rest;
     base = o * M;
     stride = 1;
   }
 
   uint32_t x[8][8];
+  if (active) {
 #pragma unroll
-  for (int r = 0; r < 8; r++) ld_fe(x[r], p.in + base + (uint64_t)(q + T * r) * stride);
+    for (int r = 0; r < 8; r++) {
+      if (BATCH)
+        ld_fe_cg(x[r], p.in + base + (uint64_t)(q + T * r) * stride);
+      else
+        ld_fe(x[r], p.in + base + (uint64_t)(q + T * r) * stride);
+    }
+  } else {
+#pragma unroll
+    for (int r = 0; r < 8; r++) set_zero(x[r]);
+  }
 
-  if (p.pre_lo) {
+  if (p.pre_lo && active) {
     const uint64_t mask = (1ull << p.pre_shift) - 1;
 #pragma unroll
     for (int r = 0; r < 8; r++) {
@@ -200,7 +201,8 @@ __global__ void __launch_bounds__(B >= 12 ? 512 : 256, B >= 12 ? 1 : ZK_NTT_MIN_
   }
   __syncthreads();
 
-  ntt_rounds<B, B>(x, q, g * M, smem, plane_stride, tws);
+  ntt_rounds<B, B>(x, q, g * M, smem, plane_stride, tws, active);
+  if (!active) return;
 
   // element r now holds output k = bitrev_B(8q + r)
   if (!p.is_final) {
@@ -241,6 +243,83 @@ __global__ void __launch_bounds__(B >= 12 ? 512 : 256, B >= 12 ? 1 : ZK_NTT_MIN_
         reduce_once<P_r>(v, x[r]);
       }
       st_fe(p.out + rev + ((uint64_t)k << total), v);
+    }
+  }
+}
+
+template <int B>
+__global__ void __launch_bounds__(256, ZK_NTT_MIN_BLOCKS) ntt_pass_kernel(const PassParams p) {
+  extern __shared__ uint32_t smem[];
+  ntt_pass_tile<B, false>(p, blockIdx.x, smem);
+}
+
+// ---------------------------------------------------------------------------
+// persistent batch kernel: the passes of many transforms in one launch
+// ---------------------------------------------------------------------------
+// Work items are CTA tiles ordered by pass level (every first pass before any
+// second pass, ...).  A CTA takes the next item with one atomic; before a
+// tile of pass t it waits for all tiles of pass t-1 of the same transform.
+// Those were handed out earlier to CTAs that are already running and never
+// wait on later items, so the waits always end; each is still bounded by a
+// clock budget after which the kernel records an error and stops.
+__device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__global__ void __launch_bounds__(256, 2) ntt_batch_kernel(const BatchPass* passes, uint32_t npass,
+                                                          uint32_t total_tiles, uint32_t* next, uint32_t* done,
+                                                          uint32_t* err, uint64_t spin_cycles) {
+  extern __shared__ uint32_t smem[];
+  __shared__ uint32_t s_w, s_k, s_stop;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      uint32_t w = atomicAdd(next, 1u);
+      s_stop = (w >= total_tiles || ld_acquire_u32(err) != 0) ? 1u : 0u;
+      if (!s_stop) {
+        // last pass whose first tile index is <= w
+        uint32_t lo = 0, hi = npass;
+        while (hi - lo > 1) {
+          const uint32_t mid = (lo + hi) / 2;
+          if (passes[mid].tile_base <= w) lo = mid; else hi = mid;
+        }
+        const BatchPass& bp = passes[lo];
+        if (bp.dep != 0xffffffffu) {
+          const uint64_t t0 = clock64();
+          while (ld_acquire_u32(done + bp.dep) < bp.dep_tiles) {
+            if (clock64() - t0 > spin_cycles) {
+              atomicExch(err, 1u);
+              s_stop = 1;
+              break;
+            }
+            __nanosleep(64);
+          }
+        }
+        s_w = w;
+        s_k = lo;
+      }
+    }
+    __syncthreads();
+    if (s_stop) return;
+    const BatchPass& bp = passes[s_k];
+    const uint64_t tile = s_w - bp.tile_base;
+    switch (bp.B) {
+      case 3: ntt_pass_tile<3, true>(bp.p, tile, smem); break;
+      case 4: ntt_pass_tile<4, true>(bp.p, tile, smem); break;
+      case 5: ntt_pass_tile<5, true>(bp.p, tile, smem); break;
+      case 6: ntt_pass_tile<6, true>(bp.p, tile, smem); break;
+      case 7: ntt_pass_tile<7, true>(bp.p, tile, smem); break;
+      case 8: ntt_pass_tile<8, true>(bp.p, tile, smem); break;
+      case 9: ntt_pass_tile<9, true>(bp.p, tile, smem); break;
+      case 10: ntt_pass_tile<10, true>(bp.p, tile, smem); break;
+      case 11: ntt_pass_tile<11, true>(bp.p, tile, smem); break;
+      default: break;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      atomicAdd(done + s_k, 1u);
     }
   }
 }
@@ -524,9 +603,62 @@ static cudaError_t dispatch_pass(int B, const PassParams& pp, uint64_t ncta, cud
     case 9: return launch_pass<9>(pp, ncta, s);
     case 10: return launch_pass<10>(pp, ncta, s);
     case 11: return launch_pass<11>(pp, ncta, s);
-    case 12: return launch_pass<12>(pp, ncta, s);
     default: return cudaErrorInvalidValue;
   }
+}
+
+uint64_t ntt_pass_params(const NttTables& t, int k, fe* d_a, fe* d_tmp, const PowTables* pre, const host::Fr* post,
+                         PassParams* out) {
+  const NttPlan& p = t.plan;
+  const int L = p.log_n;
+  int done = 0;
+  for (int j = 0; j < k; j++) done += p.bits[j];
+  const int b = p.bits[k];
+  const bool final_pass = (k + 1 == p.npass);
+  PassParams pp{};
+  pp.inner = t.inner[k];
+  pp.twist = t.twist[k];
+  pp.log_J = (uint32_t)(L - done - b);
+  pp.log_O = (uint32_t)done;
+  pp.log_m1 = (uint32_t)p.bits[0];
+  pp.nprev = final_pass ? (uint32_t)k : 0u;
+  for (int j = 0; j < k && j < NTT_MAX_PASS; j++) pp.prev_bits[j] = (uint32_t)p.bits[j];
+  pp.is_final = final_pass ? 1u : 0u;
+  if (k == 0 && pre) {
+    pp.pre_lo = pre->lo;
+    pp.pre_hi = pre->hi;
+    pp.pre_shift = pre->shift;
+  }
+  if (final_pass && post) {
+    pp.has_post = 1;
+    pp.post = to_fe_rp(*post);
+  }
+  // buffers: single pass in place; otherwise a -> tmp, tmp in place, tmp -> a
+  if (p.npass == 1) {
+    pp.in = d_a;
+    pp.out = d_a;
+  } else if (k == 0) {
+    pp.in = d_a;
+    pp.out = d_tmp;
+  } else if (!final_pass) {
+    pp.in = d_tmp;
+    pp.out = d_tmp;
+  } else {
+    pp.in = d_tmp;
+    pp.out = d_a;
+  }
+  const uint32_t Gmax = b >= 11 ? 1u : (1u << (11 - b));
+  uint64_t groups_dim;
+  if (!final_pass) {
+    groups_dim = 1ull << pp.log_J;  // columns per outer block
+  } else if (p.npass == 1) {
+    groups_dim = 1;
+  } else {
+    groups_dim = 1ull << p.bits[0];  // consecutive k_1 digits
+  }
+  pp.G = (uint32_t)std::min<uint64_t>(Gmax, groups_dim);
+  *out = pp;
+  return (1ull << (L - b)) / pp.G;
 }
 
 cudaError_t ntt_run(const NttTables& t, fe* d_a, fe* d_tmp, const PowTables* pre, const host::Fr* post, cudaStream_t s) {
@@ -539,65 +671,42 @@ cudaError_t ntt_run(const NttTables& t, fe* d_a, fe* d_tmp, const PowTables* pre
                                      pre ? pre->shift : 0u, post ? 1u : 0u, po);
     return cudaGetLastError();
   }
-  int done = 0;
+  static const char* names[12] = {"", "", "", "ntt_pass_b3", "ntt_pass_b4", "ntt_pass_b5", "ntt_pass_b6",
+                                  "ntt_pass_b7", "ntt_pass_b8", "ntt_pass_b9", "ntt_pass_b10", "ntt_pass_b11"};
   for (int k = 0; k < p.npass; k++) {
     const int b = p.bits[k];
-    const bool final_pass = (k + 1 == p.npass);
-    PassParams pp{};
-    pp.inner = t.inner[k];
-    pp.twist = t.twist[k];
-    pp.log_J = (uint32_t)(L - done - b);
-    pp.log_O = (uint32_t)done;
-    pp.log_m1 = (uint32_t)p.bits[0];
-    pp.nprev = final_pass ? (uint32_t)k : 0u;
-    for (int j = 0; j < k && j < NTT_MAX_PASS; j++) pp.prev_bits[j] = (uint32_t)p.bits[j];
-    pp.is_final = final_pass ? 1u : 0u;
-    if (k == 0 && pre) {
-      pp.pre_lo = pre->lo;
-      pp.pre_hi = pre->hi;
-      pp.pre_shift = pre->shift;
-    }
-    if (final_pass && post) {
-      pp.has_post = 1;
-      pp.post = to_fe_rp(*post);
-    }
-    // buffers: single pass in place; otherwise a -> tmp, tmp in place, tmp -> a
-    if (p.npass == 1) {
-      pp.in = d_a;
-      pp.out = d_a;
-    } else if (k == 0) {
-      pp.in = d_a;
-      pp.out = d_tmp;
-    } else if (!final_pass) {
-      pp.in = d_tmp;
-      pp.out = d_tmp;
-    } else {
-      pp.in = d_tmp;
-      pp.out = d_a;
-    }
-    const uint32_t Gmax = b >= 11 ? 1u : (1u << (11 - b));
-    uint64_t groups_dim;
-    if (!final_pass) {
-      groups_dim = 1ull << pp.log_J;                // columns per outer block
-    } else if (p.npass == 1) {
-      groups_dim = 1;
-    } else {
-      groups_dim = 1ull << p.bits[0];               // consecutive k_1 digits
-    }
-    pp.G = (uint32_t)std::min<uint64_t>(Gmax, groups_dim);
-    const uint64_t total_groups = 1ull << (L - b);
-    const uint64_t ncta = total_groups / pp.G;
-    static const char* names[13] = {"", "", "", "ntt_pass_b3", "ntt_pass_b4", "ntt_pass_b5", "ntt_pass_b6",
-                                    "ntt_pass_b7", "ntt_pass_b8", "ntt_pass_b9", "ntt_pass_b10", "ntt_pass_b11",
-                                    "ntt_pass_b12"};
+    PassParams pp;
+    const uint64_t ncta = ntt_pass_params(t, k, d_a, d_tmp, pre, post, &pp);
     const double nel = (double)(1ull << L);
     // algorithmic work: radix-2 convention (n/2) * b products; bytes: read + write (+ twist table)
-    ProfScope prof(names[b], s, nel / 2 * b, nel * 32.0 * (final_pass ? 2 : 3));
+    ProfScope prof(names[b], s, nel / 2 * b, nel * 32.0 * (pp.is_final ? 2 : 3));
     cudaError_t e = dispatch_pass(b, pp, ncta, s);
     if (e != cudaSuccess) return e;
-    done += b;
   }
   return cudaSuccess;
+}
+
+static size_t batch_smem_bytes() { return (size_t)8 * 2048 * 4 + (size_t)1024 * 32; }  // B <= 11
+
+int ntt_batch_grid(int device) {
+  static int cached[64] = {0};
+  if (device >= 0 && device < 64 && cached[device]) return cached[device];
+  cudaFuncSetAttribute(ntt_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)batch_smem_bytes());
+  int sms = 0, per_sm = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ntt_batch_kernel, 256, batch_smem_bytes());
+  const int g = sms * (per_sm > 0 ? per_sm : 1);
+  if (device >= 0 && device < 64) cached[device] = g;
+  return g;
+}
+
+cudaError_t ntt_batch_launch(const BatchPass* d_passes, uint32_t npass, uint32_t total_tiles, uint32_t* d_next,
+                             uint32_t* d_done, uint32_t* d_err, int grid, cudaStream_t s) {
+  // about two seconds at the B200 boost clock
+  const uint64_t spin_cycles = 4000000000ull;
+  ntt_batch_kernel<<<grid, 256, batch_smem_bytes(), s>>>(d_passes, npass, total_tiles, d_next, d_done, d_err,
+                                                         spin_cycles);
+  return cudaGetLastError();
 }
 
 cudaError_t fr_scale_copy(fe* dst, const fe* src, size_t n, size_t dst_stride, const PowTables* powc, cudaStream_t s) {

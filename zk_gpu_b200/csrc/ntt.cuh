@@ -63,6 +63,47 @@ cudaError_t ntt_tables_fill(NttTables* t, const host::Fr& omega, int log_n, fe* 
 // (caller frees with pow_tables_free on the same stream).
 cudaError_t pow_tables_make(PowTables* t, const host::Fr& c, int log_n, cudaStream_t s);
 void pow_tables_free(PowTables* t, cudaStream_t s);
+// Cached (device, c, log_n) power tables, owned by the cache.
+const PowTables* pow_tables_get(int device, const host::Fr& c, int log_n, cudaStream_t s, cudaError_t* err);
+
+// Parameters of one pass launch (kernel argument / batch descriptor).
+struct PassParams {
+  const fe* in;
+  fe* out;
+  const fe* inner;   // w_m^e, e < m/2 (R' form)
+  const fe* twist;   // [k * J + j], non-final passes (R' form)
+  const fe* pre_lo;  // coset powers (first pass), or null
+  const fe* pre_hi;
+  uint32_t pre_shift;
+  uint32_t log_J;
+  uint32_t log_O;
+  uint32_t log_m1;
+  uint32_t nprev;
+  uint32_t prev_bits[NTT_MAX_PASS];
+  uint32_t G;
+  uint32_t is_final;
+  uint32_t has_post;
+  fe post;  // R' form
+};
+
+// Pass k of the plan in `t` over d_a / d_tmp; returns its CTA count.
+uint64_t ntt_pass_params(const NttTables& t, int k, fe* d_a, fe* d_tmp, const PowTables* pre, const host::Fr* post,
+                         PassParams* pp);
+
+// One pass of one transform inside a batch launch.
+struct BatchPass {
+  PassParams p;
+  uint32_t B;
+  uint32_t ntiles;
+  uint32_t tile_base;  // global index of this pass's first tile
+  uint32_t dep;        // index of the pass this one waits for, or ~0u
+  uint32_t dep_tiles;  // tiles of that pass
+};
+// Launch the persistent batch kernel over `npass` descriptors (device memory,
+// ordered by level), with counters next/done/err zeroed by the caller.
+cudaError_t ntt_batch_launch(const BatchPass* d_passes, uint32_t npass, uint32_t total_tiles, uint32_t* d_next,
+                             uint32_t* d_done, uint32_t* d_err, int grid, cudaStream_t s);
+int ntt_batch_grid(int device);
 
 // Runs the NTT over d_a (2^log_n elements, in place).  d_tmp is scratch of
 // the same size (unused for single-pass plans).  pre (nullable) applies the
