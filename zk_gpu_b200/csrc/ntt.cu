@@ -620,7 +620,9 @@ uint64_t ntt_pass_params(const NttTables& t, int k, fe* d_a, fe* d_tmp, const Po
   pp.twist = t.twist[k];
   pp.log_J = (uint32_t)(L - done - b);
   pp.log_O = (uint32_t)done;
-  pp.log_m1 = (uint32_t)p.bits[0];
+  // final-pass grouping runs over consecutive first digits k_1; a single-pass
+  // plan has no digits (one group, rest_count = 1)
+  pp.log_m1 = p.npass > 1 ? (uint32_t)p.bits[0] : 0u;
   pp.nprev = final_pass ? (uint32_t)k : 0u;
   for (int j = 0; j < k && j < NTT_MAX_PASS; j++) pp.prev_bits[j] = (uint32_t)p.bits[j];
   pp.is_final = final_pass ? 1u : 0u;
