@@ -301,6 +301,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     del d_sc, d_bs
 
     batched = bench_batched(zk, torch, dev, stream, args.steps)
+    serving = bench_serving(zk, torch, dev) if not args.no_serving else None
 
     # ---- e2e through the host-buffer C ABI, pinned host memory ----
     h_vals = torch.from_numpy(vals_np.view(np.int64)).pin_memory()
@@ -356,7 +357,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                   "msm_2p22_ms": round(msm_ms, 3),
                   "msm_kernels": {k: {"launches": v["launches"], "ms": round(v["ms"], 3)} for k, v in msm_prof.items()},
                   "msm_roofline": msm_roofline(msm_prof, imad_ps, n_msm, msm_ms),
-                  "batched_ntt": batched},
+                  "batched_ntt": batched,
+                  "serving": serving},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         t, threads = cpu_lde_sample()
@@ -441,6 +443,165 @@ def bench_batched(zk, torch, dev: int, stream, steps: int, njobs: int = 512, see
             "launches_per_run": {"batched": batch_launches, "one_call_per_job": single_launches},
             "work_items": info["tiles"], "passes": info["passes"], "grid": info["grid"],
             "inputs": "uniform 252-bit values (< r) from torch.randint on the device"}
+
+
+def serving_trace(njobs: int, rate: float, seed: int = 99):
+    """(arrival_s, kind, log_size) per job: Poisson arrivals; 70% NTT / coset
+    LDE (log2 size uniform 12..22, half each), 30% MSM (log2 points 14..20)."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, njobs))
+    out = []
+    for i in range(njobs):
+        u = rng.random()
+        if u < 0.35:
+            out.append((float(t[i]), "ntt", int(rng.integers(12, 23))))
+        elif u < 0.70:
+            out.append((float(t[i]), "lde", int(rng.integers(12, 23))))
+        else:
+            out.append((float(t[i]), "msm", int(rng.integers(14, 21))))
+    return out
+
+
+def bench_serving(zk, torch, dev: int, njobs: int = 1000, rate: float = 2000.0):
+    """Serving loop (continuous batching) vs one call per job on the same GPU,
+    same arrival trace; host buffers pinned, shared per size class (read-only
+    inputs; outputs of identical jobs are identical)."""
+    import ctypes
+    trace = serving_trace(njobs, rate)
+    pools = {}
+
+    def pinned(rows, cols):
+        t = torch.empty((rows, cols), dtype=torch.int64).pin_memory()
+        return t, t.numpy().view(np.uint64)
+
+    consts = {}
+    for k in range(12, 25):
+        w = root_of_unity(k)
+        consts[k] = dict(omega=mont(w), omega_inv=mont(pow(w, -1, R_MOD)), divisor=mont(pow(1 << k, -1, R_MOD)))
+    g7 = mont(7)
+    for _, kind, k in trace:
+        key = (kind, k)
+        if key in pools:
+            continue
+        if kind == "msm":
+            ti, a = pinned(1 << k, 4)
+            a[:] = rand_fr(1 << k, k)
+            to, o = pinned(1, 12)
+        else:
+            ti, a = pinned(1 << k, 4)
+            a[:] = rand_fr(1 << k, 1000 + k)
+            to, o = pinned(1 << (k + 2 if kind == "lde" else k), 4)
+        pools[key] = (ti, a, to, o)
+    nb = 1 << 20
+    bases = gen_bases_tiled(nb)
+
+    def make_job(kind, k):
+        ti, a, to, o = pools[(kind, k)]
+        if kind == "ntt":
+            return zk.ntt_job(a, o, k, consts[k]["omega"])
+        if kind == "lde":
+            return zk.lde_job(a, o, k, k + 2, consts[k]["omega_inv"], consts[k]["divisor"], g7,
+                              consts[k + 2]["omega"])
+        return zk.msm_job(a, o, 1 << k, bid)
+
+    def pct(x, q):
+        return float(np.percentile(np.asarray(x), q)) if len(x) else None
+
+    # ---- serving loop ----
+    srv = zk.Server(device=dev, hbm_budget=150 * 10**9)
+    bid = srv.add_bases(bases)
+
+    def run_server(open_loop: bool):
+        lats = [None] * len(trace)
+        tickets = [None] * len(trace)
+        done_evt = threading.Event()
+
+        def waiter():
+            for i in range(len(trace)):
+                while tickets[i] is None:
+                    time.sleep(0.0002)
+                lats[i] = srv.wait(tickets[i]) / 1e3
+            done_evt.set()
+
+        th = threading.Thread(target=waiter)
+        th.start()
+        t0 = time.perf_counter()
+        jobs_keep = []
+        for i, (at, kind, k) in enumerate(trace):
+            if open_loop:
+                d = t0 + at - time.perf_counter()
+                if d > 0:
+                    time.sleep(d)
+            j = make_job(kind, k)
+            jobs_keep.append(j)
+            tickets[i] = srv.submit(j)
+        done_evt.wait()
+        th.join()
+        span = time.perf_counter() - t0
+        return lats, span
+
+    run_server(False)  # warm-up: tables, pools, allocator
+    lat_s, span_s = run_server(True)
+    lat_sc, span_sc = run_server(False)
+    st = srv.stats()
+    # ---- one call per job (synchronous, one job at a time, same residency) ----
+    stream = torch.cuda.Stream(device=dev)
+    d_bases = torch.from_numpy(bases.view(np.int64)).to(f"cuda:{dev}")
+    d_out = torch.zeros(12, dtype=torch.int64, device=f"cuda:{dev}")
+
+    def one_call(kind, k):
+        ti, a, to, o = pools[(kind, k)]
+        with torch.cuda.stream(stream):
+            if kind == "ntt":
+                d = ti.to(f"cuda:{dev}", non_blocking=True)
+                zk.ntt_dev(d, k, consts[k]["omega"], stream=stream)
+                to.copy_(d, non_blocking=True)
+            elif kind == "lde":
+                d = ti.to(f"cuda:{dev}", non_blocking=True)
+                e = torch.empty((1 << (k + 2), 4), dtype=torch.int64, device=f"cuda:{dev}")
+                zk.lagrange_to_extended_dev(d, e, k, k + 2, consts[k]["omega_inv"], consts[k]["divisor"], g7,
+                                            consts[k + 2]["omega"], stream=stream)
+                to.copy_(e, non_blocking=True)
+            else:
+                d = ti.to(f"cuda:{dev}", non_blocking=True)
+                zk.msm_dev(d, d_bases[: 1 << k], d_out, stream=stream)
+                to.copy_(d_out.view(1, 12), non_blocking=True)
+        stream.synchronize()
+
+    def run_plain(open_loop: bool):
+        lats = []
+        t0 = time.perf_counter()
+        for at, kind, k in trace:
+            if open_loop:
+                d = t0 + at - time.perf_counter()
+                if d > 0:
+                    time.sleep(d)
+            arrive = t0 + at if open_loop else t0
+            one_call(kind, k)
+            lats.append(time.perf_counter() - arrive)
+        return lats, time.perf_counter() - t0
+
+    for kind, k in pools:
+        one_call(kind, k)
+    lat_p, span_p = run_plain(True)
+    lat_pc, span_pc = run_plain(False)
+    srv.close()
+    n = len(trace)
+    return {
+        "jobs": n, "offered_rate_jobs_s": rate, "mix": "35% NTT 2^12-2^22, 35% coset LDE x4 2^12-2^22, "
+                                                         "30% MSM 2^14-2^20 (resident bases)",
+        "open_loop": {
+            "batched": {"jobs_s": round(n / span_s, 1), "p50_ms": round(pct(lat_s, 50) * 1e3, 3),
+                        "p99_ms": round(pct(lat_s, 99) * 1e3, 3)},
+            "one_call_per_job": {"jobs_s": round(n / span_p, 1), "p50_ms": round(pct(lat_p, 50) * 1e3, 3),
+                                 "p99_ms": round(pct(lat_p, 99) * 1e3, 3)}},
+        "closed_loop_saturation": {
+            "batched_jobs_s": round(n / span_sc, 1), "one_call_per_job_jobs_s": round(n / span_pc, 1),
+            "speedup": round(span_pc / span_sc, 3),
+            "batched_p99_ms": round(pct(lat_sc, 99) * 1e3, 3), "one_call_p99_ms": round(pct(lat_pc, 99) * 1e3, 3)},
+        "server": {"waves": st["waves"], "batch_launches": st["batch_launches"], "hbm_peak_gb":
+                   round(st["hbm_peak"] / 1e9, 2), "rejected": st["rejected"], "failed": st["failed"]},
+    }
 
 
 def small_fr(n: int, seed: int, bits: int = 16) -> np.ndarray:
@@ -555,6 +716,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving-loop sub-benchmark")
     ap.add_argument("--case", choices=["ntt22", "ntt24", "lde20", "msm20"], default=None,
                     help="run a small profiling case instead of the benchmark")
     args = ap.parse_args()

@@ -157,6 +157,58 @@ void zkgpu_ntt_batch_info(void *handle, uint32_t *passes, uint32_t *tiles, int *
 void zkgpu_ntt_batch_destroy(void *handle);
 
 /* ======================================================================
+ * Serving loop: continuous batching with HBM-budget admission.  Replaces the
+ * reference's GpuLock / get_gpu / THREAD_POOL scheduling
+ * (src/gpulock.rs:72-246, src/config.rs:97-127, src/threadpool.rs:34-121).
+ * Jobs arrive with host input/output buffers (pinned memory keeps every copy
+ * asynchronous); admitted NTT/LDE jobs of one scheduling wave run as one
+ * persistent batch launch, MSMs run against resident bases.
+ * ====================================================================== */
+#define ZKGPU_KIND_NTT 0u /* in place on `output` (input copied from `input`) */
+#define ZKGPU_KIND_LDE 1u /* lagrange 2^log_n -> coset extended 2^log_ext */
+#define ZKGPU_KIND_MSM 2u /* sum scalars[i] * bases[i], i < n, over a resident base set */
+typedef struct {
+    uint32_t kind;
+    uint32_t log_n;      /* NTT / LDE input size */
+    uint32_t log_ext;    /* LDE only */
+    uint32_t flags;      /* NTT: ZKGPU_JOB_COSET / ZKGPU_JOB_SCALE */
+    uint64_t n;          /* MSM: points */
+    uint32_t bases_id;   /* MSM: id from zkgpu_server_add_bases */
+    uint32_t reserved;
+    const uint64_t *input;  /* NTT/LDE: 2^log_n elements; MSM: n scalars */
+    uint64_t *output;       /* NTT: 2^log_n; LDE: 2^log_ext; MSM: 12 words (normalised Jacobian) */
+    uint64_t omega[4];      /* NTT: root; LDE: omega_inv of the 2^log_n domain */
+    uint64_t coset[4];      /* NTT: coset c; LDE: coset generator g */
+    uint64_t scale[4];      /* NTT: output scale; LDE: divisor n^-1 */
+    uint64_t omega_ext[4];  /* LDE: root of the 2^log_ext domain */
+} zkgpu_job;
+
+typedef struct {
+    uint64_t submitted, rejected, completed, failed;
+    uint64_t waves, batch_launches;
+    uint64_t hbm_budget, hbm_used, hbm_peak;
+    uint64_t pending, inflight;
+} zkgpu_server_stats;
+
+/* device memory a job needs while in flight (bytes) */
+uint64_t zkgpu_job_footprint(const zkgpu_job *job);
+/* Admission policy, simulated on the host (no device): jobs with the given
+ * footprints arrive in order; `admit_rounds[i]` receives the scheduling round
+ * in which job i is admitted when every admitted job completes one round
+ * after admission (-1 = rejected).  Returns the peak bytes in use. */
+uint64_t zkgpu_admission_simulate(uint64_t budget, const uint64_t *footprints, uint32_t n, int32_t *admit_rounds);
+
+int zkgpu_server_create(int device, uint64_t hbm_budget_bytes, uint32_t max_wave_jobs, void **server);
+/* upload a base set once (affine, 8 words per point); it stays resident */
+int zkgpu_server_add_bases(void *server, const uint64_t *bases_xy, uint64_t n, uint32_t *bases_id);
+/* non-blocking; ZKGPU_EADMIT if the job can never fit the budget */
+int zkgpu_server_submit(void *server, const zkgpu_job *job, uint64_t *ticket);
+/* wait for a job (timeout_ms 0 = forever); *latency_ms = completion - submit */
+int zkgpu_server_wait(void *server, uint64_t ticket, uint32_t timeout_ms, double *latency_ms);
+int zkgpu_server_stats_get(void *server, zkgpu_server_stats *out);
+void zkgpu_server_destroy(void *server);
+
+/* ======================================================================
  * Diagnostics.
  * ====================================================================== */
 /* elementwise field op on host arrays through the device kernels:

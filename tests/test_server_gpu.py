@@ -1,0 +1,113 @@
+"""GPU: the serving loop.  A mix of NTT, coset-LDE and MSM jobs submitted
+together (continuous batching, waves overlapping on the device) gives, for
+every job, exactly the result of the same job run alone, and the oracle's."""
+import threading
+
+import numpy as np
+import pytest
+
+from oracle import bigref as B
+
+pytestmark = pytest.mark.gpu
+
+
+def test_server_mix_matches_alone(zk, oracle):
+    rng = np.random.default_rng(11)
+    srv = zk.Server(device=0, hbm_budget=8 * 10**9)
+    bases, k = oracle.rand_bases(1 << 14, 5, with_dlog=True)
+    bid = srv.add_bases(bases)
+    jobs = []
+    for i in range(40):
+        kind = int(rng.integers(0, 3))
+        if kind == 0:
+            lg = int(rng.integers(3, 17))
+            a = oracle.rand_fr(1 << lg, 300 + i)
+            out = np.zeros_like(a)
+            w = oracle.omega(lg)
+            coset = oracle.to_mont(7) if rng.integers(0, 2) else None
+            jb = zk.ntt_job(a, out, lg, w, coset=coset)
+            alone = zk.coset_fft(a, w, lg, coset) if coset is not None else zk.fft(a, w, lg)
+            ref = oracle.best_fft(oracle.distribute_powers(a, coset) if coset is not None else a, w, lg)
+            jobs.append((jb, a, out, alone, ref))
+        elif kind == 1:
+            lg = int(rng.integers(3, 15))
+            a = oracle.rand_fr(1 << lg, 400 + i)
+            out = np.zeros((1 << (lg + 2), 4), np.uint64)
+            wi, d = oracle.inv(oracle.omega(lg)), oracle.inv(oracle.to_mont(1 << lg))
+            g, we = oracle.to_mont(7), oracle.omega(lg + 2)
+            jb = zk.lde_job(a, out, lg, lg + 2, wi, d, g, we)
+            alone = zk.lagrange_to_extended(a, lg, lg + 2, wi, d, g, we)
+            ref = oracle.coeff_to_extended(oracle.ifft(a, wi, lg, d), lg, lg + 2, g, we)
+            jobs.append((jb, a, out, alone, ref))
+        else:
+            n = int(rng.integers(1, 1 << 14))
+            s = oracle.rand_fr(n, 500 + i)
+            out = np.zeros(12, np.uint64)
+            jb = zk.msm_job(s, out, n, bid)
+            alone = zk.msm(s, bases[:n])
+            ref = oracle.msm_by_dlog(s, k[:n])
+            jobs.append((jb, s, out, alone, ref))
+    tickets = [srv.submit(j[0]) for j in jobs]
+    lats = [srv.wait(t, timeout_ms=120000) for t in tickets]
+    for (jb, _, out, alone, ref), lat in zip(jobs, lats):
+        if jb.kind == zk.KIND_MSM:
+            aff = out[:8] if out[8:].any() else np.zeros(8, np.uint64)
+            assert np.array_equal(out, alone)
+            assert np.array_equal(aff, ref)
+        else:
+            assert np.array_equal(out, alone)
+            assert np.array_equal(out, ref)
+        assert lat > 0
+    st = srv.stats()
+    assert st["completed"] == len(jobs) and st["failed"] == 0
+    assert st["hbm_peak"] <= st["hbm_budget"]
+    srv.close()
+
+
+def test_server_admission_rejects_and_drains(zk, oracle):
+    srv = zk.Server(device=0, hbm_budget=64 * 2**20)   # 64 MiB
+    big = np.zeros((1 << 20, 4), np.uint64)           # 2^20 NTT needs 64 MiB + scratch
+    job = zk.ntt_job(big, big, 20, oracle.omega(20))
+    with pytest.raises(zk.ZkGpuError) as e:
+        srv.submit(job)
+    assert e.value.code == zk.EADMIT
+    # many small jobs under a tight budget still all complete
+    outs, tickets = [], []
+    for i in range(30):
+        a = oracle.rand_fr(1 << 16, 700 + i)
+        o = np.zeros_like(a)
+        tickets.append(srv.submit(zk.ntt_job(a, o, 16, oracle.omega(16)), keep=a))
+        outs.append((a, o))
+    for t in tickets:
+        srv.wait(t, timeout_ms=60000)
+    for a, o in outs:
+        assert np.array_equal(o, oracle.best_fft(a, oracle.omega(16), 16))
+    st = srv.stats()
+    assert st["rejected"] == 1 and st["completed"] == 30 and st["hbm_peak"] <= st["hbm_budget"]
+    srv.close()
+
+
+def test_server_concurrent_submitters(zk, oracle):
+    srv = zk.Server(device=0, hbm_budget=4 * 10**9)
+    errors = []
+
+    def worker(seed):
+        try:
+            for i in range(5):
+                lg = 10 + (seed + i) % 6
+                a = oracle.rand_fr(1 << lg, seed * 100 + i)
+                o = np.zeros_like(a)
+                t = srv.submit(zk.ntt_job(a, o, lg, oracle.omega(lg)), keep=a)
+                srv.wait(t, timeout_ms=60000)
+                if not np.array_equal(o, oracle.best_fft(a, oracle.omega(lg), lg)):
+                    errors.append((seed, i))
+        except Exception as ex:  # pragma: no cover
+            errors.append(repr(ex))
+
+    th = [threading.Thread(target=worker, args=(s,)) for s in range(6)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    assert not errors
+    srv.close()

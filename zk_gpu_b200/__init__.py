@@ -71,6 +71,14 @@ EXPORTS = {
     "zkgpu_ntt_batch_check": (_i32, [P]),
     "zkgpu_ntt_batch_info": (None, [P, P, P, P]),
     "zkgpu_ntt_batch_destroy": (None, [P]),
+    "zkgpu_job_footprint": (_u64, [P]),
+    "zkgpu_admission_simulate": (_u64, [_u64, P, _u32, P]),
+    "zkgpu_server_create": (_i32, [_i32, _u64, _u32, P]),
+    "zkgpu_server_add_bases": (_i32, [P, P, _u64, P]),
+    "zkgpu_server_submit": (_i32, [P, P, P]),
+    "zkgpu_server_wait": (_i32, [P, _u64, _u32, P]),
+    "zkgpu_server_stats_get": (_i32, [P, P]),
+    "zkgpu_server_destroy": (None, [P]),
     "zkgpu_field_op": (_i32, [_i32, _i32, _i32, P, P, P, _u64]),
     "zkgpu_last_error": (ctypes.c_char_p, []),
     "zkgpu_launch_count": (_u64, [_i32]),
@@ -311,6 +319,117 @@ class NttBatch:
             self.close()
         except Exception:
             pass
+
+
+KIND_NTT, KIND_LDE, KIND_MSM = 0, 1, 2
+
+
+class Job(ctypes.Structure):
+    """zkgpu_job (include/zkgpu.h)"""
+    _fields_ = [("kind", ctypes.c_uint32), ("log_n", ctypes.c_uint32), ("log_ext", ctypes.c_uint32),
+                ("flags", ctypes.c_uint32), ("n", ctypes.c_uint64), ("bases_id", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32), ("input", ctypes.c_void_p), ("output", ctypes.c_void_p),
+                ("omega", ctypes.c_uint64 * 4), ("coset", ctypes.c_uint64 * 4), ("scale", ctypes.c_uint64 * 4),
+                ("omega_ext", ctypes.c_uint64 * 4)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_uint64) for k in ("submitted", "rejected", "completed", "failed", "waves",
+                                               "batch_launches", "hbm_budget", "hbm_used", "hbm_peak", "pending",
+                                               "inflight")]
+
+
+def _set4(dst, v):
+    dst[:] = [int(x) for x in _el(v)]
+
+
+def ntt_job(inp: np.ndarray, out: np.ndarray, log_n: int, omega, coset=None, scale=None) -> Job:
+    j = Job()
+    j.kind, j.log_n = KIND_NTT, log_n
+    j.input, j.output = inp.ctypes.data, out.ctypes.data
+    _set4(j.omega, omega)
+    if coset is not None:
+        j.flags |= JOB_COSET
+        _set4(j.coset, coset)
+    if scale is not None:
+        j.flags |= JOB_SCALE
+        _set4(j.scale, scale)
+    return j
+
+
+def lde_job(inp: np.ndarray, out: np.ndarray, log_n: int, log_ext: int, omega_inv, divisor, g, omega_ext) -> Job:
+    j = Job()
+    j.kind, j.log_n, j.log_ext = KIND_LDE, log_n, log_ext
+    j.input, j.output = inp.ctypes.data, out.ctypes.data
+    _set4(j.omega, omega_inv)
+    _set4(j.scale, divisor)
+    _set4(j.coset, g)
+    _set4(j.omega_ext, omega_ext)
+    return j
+
+
+def msm_job(scalars: np.ndarray, out: np.ndarray, n: int, bases_id: int) -> Job:
+    j = Job()
+    j.kind, j.n, j.bases_id = KIND_MSM, n, bases_id
+    j.input, j.output = scalars.ctypes.data, out.ctypes.data
+    return j
+
+
+class Server:
+    """Serving loop (continuous batching, HBM-budget admission) over the C ABI.
+    Host buffers passed to submit() must stay alive until wait() returns."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 150 * 10**9, max_wave_jobs: int = 4096):
+        self.handle = ctypes.c_void_p()
+        _check(lib().zkgpu_server_create(device, hbm_budget, max_wave_jobs, ctypes.byref(self.handle)),
+               "server_create")
+        self._keep = {}
+
+    def add_bases(self, bases: np.ndarray) -> int:
+        b = _arr(bases, 8)
+        bid = ctypes.c_uint32()
+        _check(lib().zkgpu_server_add_bases(self.handle, b.ctypes.data, b.shape[0], ctypes.byref(bid)), "add_bases")
+        return bid.value
+
+    def submit(self, job: Job, keep=None) -> int:
+        t = ctypes.c_uint64()
+        _check(lib().zkgpu_server_submit(self.handle, ctypes.byref(job), ctypes.byref(t)), "server_submit")
+        self._keep[t.value] = (job, keep)
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = 0) -> float:
+        lat = ctypes.c_double()
+        rc = lib().zkgpu_server_wait(self.handle, ticket, timeout_ms, ctypes.byref(lat))
+        self._keep.pop(ticket, None)
+        _check(rc, "server_wait")
+        return lat.value
+
+    def stats(self) -> dict:
+        s = ServerStats()
+        _check(lib().zkgpu_server_stats_get(self.handle, ctypes.byref(s)), "server_stats")
+        return {k: getattr(s, k) for k, _ in ServerStats._fields_}
+
+    def close(self):
+        if self.handle:
+            lib().zkgpu_server_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def job_footprint(job: Job) -> int:
+    return int(lib().zkgpu_job_footprint(ctypes.byref(job)))
+
+
+def admission_simulate(budget: int, footprints) -> tuple:
+    fp = np.ascontiguousarray(footprints, dtype=np.uint64)
+    rounds = np.zeros(fp.shape[0], np.int32)
+    peak = lib().zkgpu_admission_simulate(budget, fp.ctypes.data, fp.shape[0], rounds.ctypes.data)
+    return int(peak), rounds
 
 
 def msm_dev(scalars, bases, out, stream=None):

@@ -1,0 +1,519 @@
+// server.cu — the serving loop: continuous batching of NTT / LDE / MSM jobs
+// on one GPU with HBM-budget admission (declared in include/zkgpu.h).
+//
+// Threads: callers submit (non-blocking) and wait; a scheduler thread admits
+// jobs in arrival order while they fit the budget and launches everything it
+// admitted as one "wave": all NTT and LDE passes of the wave go into a single
+// persistent batch launch (ntt_batch_kernel), MSMs run on a second stream
+// against resident base sets; copies are enqueued on the same streams.  A
+// completion thread retires waves in order, releases their memory to the
+// budget (which wakes the scheduler: new arrivals are admitted while earlier
+// waves still run, so their work overlaps on the device) and wakes waiters.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "admission.hpp"
+#include "host_field.hpp"
+#include "msm.cuh"
+#include "ntt.cuh"
+#include "runtime.cuh"
+
+namespace zk {
+
+namespace {
+using clk = std::chrono::steady_clock;
+
+uint64_t msm_scratch_bytes(uint64_t n) {
+  if (n == 0) return 256;
+  const MsmPlan p = make_msm_plan(n);
+  const uint64_t total = (uint64_t)p.windows * p.buckets;
+  const uint64_t entries = n * p.windows;
+  const uint64_t max_sub = entries / 64 + total + 1;
+  return total * 4 * 6 + entries * 4 + max_sub * (4 + 128) + total * 128 * 2 + 4096;
+}
+
+host::Fr fr_of(const uint64_t v[4]) {
+  host::Fr r;
+  std::memcpy(r.v, v, 32);
+  return r;
+}
+
+struct JobRec {
+  uint64_t ticket = 0;
+  zkgpu_job job{};
+  uint64_t bytes = 0;
+  clk::time_point t_submit, t_done;
+  int status = -1;  // -1 in progress
+  uint64_t* msm_out = nullptr;  // slot in the wave's pinned mailbox
+};
+
+struct Wave {
+  std::vector<JobRec*> jobs;
+  cudaStream_t s_ntt = nullptr, s_msm = nullptr;
+  cudaEvent_t ev_ntt = nullptr, ev_msm = nullptr;
+  std::vector<BatchPass> passes;  // host copy kept alive for the async upload
+  uint64_t* mailbox = nullptr;    // pinned: [0] batch error flag, then 12 words per MSM job
+  int status = ZKGPU_OK;
+};
+
+struct BaseSet {
+  fe* d = nullptr;
+  uint64_t n = 0;
+};
+
+}  // namespace
+
+class Server {
+ public:
+  Server(int dev, uint64_t budget, uint32_t max_wave) : device_(dev), adm_(budget), max_wave_(max_wave ? max_wave : 4096) {}
+
+  int start() {
+    ZK_TRY("cudaSetDevice", cudaSetDevice(device_));
+    for (int i = 0; i < kStreams; i++) {
+      ZK_TRY("cudaStreamCreate", cudaStreamCreateWithFlags(&s_ntt_[i], cudaStreamNonBlocking));
+      ZK_TRY("cudaStreamCreate", cudaStreamCreateWithFlags(&s_msm_[i], cudaStreamNonBlocking));
+    }
+    grid_ = ntt_batch_grid(device_);
+    // one pinned mailbox per stream slot; a slot is reused only after the
+    // wave that used it retired (waves retire in launch order)
+    slot_words_ = 2 + 12 * (uint64_t)max_wave_;
+    ZK_TRY("cudaMallocHost(mailbox)", cudaMallocHost((void**)&mailbox_, kStreams * slot_words_ * 8));
+    sched_ = std::thread([this] { sched_loop(); });
+    comp_ = std::thread([this] { comp_loop(); });
+    return ZKGPU_OK;
+  }
+
+  ~Server() {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      stop_ = true;
+    }
+    cv_sched_.notify_all();
+    cv_comp_.notify_all();
+    if (sched_.joinable()) sched_.join();
+    if (comp_.joinable()) comp_.join();
+    cudaSetDevice(device_);
+    cudaDeviceSynchronize();
+    for (auto& b : bases_) cudaFree(b.d);
+    if (mailbox_) cudaFreeHost(mailbox_);
+    for (int i = 0; i < kStreams; i++) {
+      if (s_ntt_[i]) cudaStreamDestroy(s_ntt_[i]);
+      if (s_msm_[i]) cudaStreamDestroy(s_msm_[i]);
+    }
+  }
+
+  int add_bases(const uint64_t* xy, uint64_t n, uint32_t* id) {
+    const uint64_t bytes = n * 64;
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      if (!adm_.reserve(bytes)) return ZKGPU_EADMIT;
+      peak_ = std::max(peak_, adm_.used() + adm_.reserved());
+    }
+    ZK_TRY("cudaSetDevice", cudaSetDevice(device_));
+    BaseSet b;
+    b.n = n;
+    ZK_TRY("cudaMalloc(bases)", cudaMalloc((void**)&b.d, std::max<uint64_t>(bytes, 64)));
+    ZK_TRY("bases H2D", cudaMemcpy(b.d, xy, bytes, cudaMemcpyHostToDevice));
+    std::lock_guard<std::mutex> lk(mu_);
+    bases_.push_back(b);
+    *id = (uint32_t)bases_.size() - 1;
+    return ZKGPU_OK;
+  }
+
+  int submit(const zkgpu_job* job, uint64_t* ticket) {
+    auto rec = std::make_unique<JobRec>();
+    rec->job = *job;
+    rec->bytes = zkgpu_job_footprint(job);
+    rec->t_submit = clk::now();
+    std::lock_guard<std::mutex> lk(mu_);
+    if (stop_) return ZKGPU_EBUSY;
+    rec->ticket = next_ticket_++;
+    submitted_++;
+    if (job->kind == ZKGPU_KIND_MSM && (job->bases_id >= bases_.size() || job->n > bases_[job->bases_id].n)) {
+      rejected_++;
+      return ZKGPU_EINVAL;
+    }
+    if (!adm_.push(rec->ticket, rec->bytes)) {
+      rejected_++;
+      return ZKGPU_EADMIT;
+    }
+    *ticket = rec->ticket;
+    jobs_.emplace(rec->ticket, std::move(rec));
+    cv_sched_.notify_one();
+    return ZKGPU_OK;
+  }
+
+  int wait(uint64_t ticket, uint32_t timeout_ms, double* latency_ms) {
+    std::unique_lock<std::mutex> lk(mu_);
+    auto it = jobs_.find(ticket);
+    if (it == jobs_.end()) return ZKGPU_EINVAL;
+    JobRec* r = it->second.get();
+    auto done = [&] { return r->status >= 0; };
+    if (timeout_ms == 0)
+      cv_done_.wait(lk, done);
+    else if (!cv_done_.wait_for(lk, std::chrono::milliseconds(timeout_ms), done))
+      return ZKGPU_ETIMEOUT;
+    if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
+    const int st = r->status;
+    jobs_.erase(it);
+    return st;
+  }
+
+  void stats(zkgpu_server_stats* o) {
+    std::lock_guard<std::mutex> lk(mu_);
+    o->submitted = submitted_;
+    o->rejected = rejected_;
+    o->completed = completed_;
+    o->failed = failed_;
+    o->waves = waves_;
+    o->batch_launches = batch_launches_;
+    o->hbm_budget = adm_.budget() + adm_.reserved();
+    o->hbm_used = adm_.used() + adm_.reserved();
+    o->hbm_peak = peak_;
+    o->pending = adm_.pending();
+    o->inflight = inflight_jobs_;
+  }
+
+ private:
+  static constexpr int kStreams = 4;
+
+  void sched_loop() {
+    cudaSetDevice(device_);
+    int rr = 0;
+    for (;;) {
+      std::vector<JobRec*> batch;
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_sched_.wait(lk, [&] { return stop_ || (adm_.pending() > 0 && waves_inflight_ < kStreams); });
+        if (stop_) return;
+        const uint64_t gen = retired_gen_;
+        for (uint64_t t : adm_.admit(max_wave_)) batch.push_back(jobs_.at(t).get());
+        peak_ = std::max(peak_, adm_.used() + adm_.reserved());
+        if (batch.empty()) {
+          // the head does not fit yet: wait until a wave retires and frees memory
+          cv_sched_.wait(lk, [&] { return stop_ || retired_gen_ != gen; });
+          continue;
+        }
+        inflight_jobs_ += batch.size();
+        waves_inflight_++;
+      }
+      auto w = std::make_unique<Wave>();
+      w->jobs = batch;
+      w->s_ntt = s_ntt_[rr];
+      w->s_msm = s_msm_[rr];
+      w->mailbox = mailbox_ + rr * slot_words_;
+      rr = (rr + 1) % kStreams;
+      launch_wave(*w);
+      {
+        std::lock_guard<std::mutex> lk(mu_);
+        waves_++;
+        inflight_.push_back(std::move(w));
+      }
+      cv_comp_.notify_one();
+    }
+  }
+
+  // Enqueue one wave: allocations, uploads, one batch launch, MSMs, downloads.
+  void launch_wave(Wave& w) {
+    cudaError_t e = cudaSuccess;
+    auto ok = [&](cudaError_t x) {
+      if (e == cudaSuccess && x != cudaSuccess) e = x;
+      return e == cudaSuccess;
+    };
+    cudaEventCreateWithFlags(&w.ev_ntt, cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&w.ev_msm, cudaEventDisableTiming);
+    w.mailbox[0] = 0;
+    uint64_t* next_msm_slot = w.mailbox + 2;
+    struct NttItem {
+      const NttTables* t;
+      fe* data;
+      fe* tmp;
+      const PowTables* pre;
+      host::Fr post;
+      bool has_post;
+      int level0;
+      int dep_job;  // index in items of the transform this one follows, or -1
+    };
+    std::vector<NttItem> items;
+    std::vector<std::pair<JobRec*, fe*>> ntt_outputs;  // device result -> job
+    std::vector<void*> frees_ntt, frees_msm;
+    for (JobRec* r : w.jobs) {
+      const zkgpu_job& j = r->job;
+      if (j.kind == ZKGPU_KIND_MSM) {
+        fe *ds = nullptr, *dout = nullptr;
+        const BaseSet& bs = bases_[j.bases_id];
+        if (ok(cudaMallocAsync((void**)&ds, std::max<uint64_t>(j.n, 1) * 32, w.s_msm)) &&
+            ok(cudaMallocAsync((void**)&dout, 96, w.s_msm)) &&
+            ok(cudaMemcpyAsync(ds, j.input, j.n * 32, cudaMemcpyHostToDevice, w.s_msm))) {
+          uint64_t nl = 0;
+          ok(msm_run(ds, bs.d, j.n, dout, w.s_msm, 0, &nl));
+          r->msm_out = next_msm_slot;
+          next_msm_slot += 12;
+          ok(cudaMemcpyAsync(r->msm_out, dout, 96, cudaMemcpyDeviceToHost, w.s_msm));
+        }
+        frees_msm.push_back(ds);
+        frees_msm.push_back(dout);
+        continue;
+      }
+      const bool lde = j.kind == ZKGPU_KIND_LDE;
+      const uint32_t L = lde ? j.log_ext : j.log_n;
+      const size_t N = (size_t)1 << L, n = (size_t)1 << j.log_n;
+      fe *d = nullptr, *tmp = nullptr;
+      if (!ok(cudaMallocAsync((void**)&d, N * 32, w.s_ntt)) || !ok(cudaMallocAsync((void**)&tmp, N * 32, w.s_ntt)))
+        break;
+      frees_ntt.push_back(d);
+      frees_ntt.push_back(tmp);
+      ok(cudaMemcpyAsync(d, j.input, n * 32, cudaMemcpyHostToDevice, w.s_ntt));
+      if (N > n) ok(cudaMemsetAsync(d + n, 0, (N - n) * 32, w.s_ntt));
+      cudaError_t te;
+      if (!lde) {
+        NttItem it{};
+        it.t = ntt_tables_get(device_, fr_of(j.omega), (int)j.log_n, w.s_ntt, &te);
+        if (!it.t) {
+          ok(te);
+          break;
+        }
+        if (j.flags & ZKGPU_JOB_COSET) it.pre = pow_tables_get(device_, fr_of(j.coset), (int)j.log_n, w.s_ntt, &te);
+        if ((j.flags & ZKGPU_JOB_COSET) && !it.pre) {
+          ok(te);
+          break;
+        }
+        it.has_post = (j.flags & ZKGPU_JOB_SCALE) != 0;
+        it.post = fr_of(j.scale);
+        it.data = d;
+        it.tmp = tmp;
+        it.level0 = 0;
+        it.dep_job = -1;
+        items.push_back(it);
+      } else {
+        NttItem a{}, b{};
+        a.t = ntt_tables_get(device_, fr_of(j.omega), (int)j.log_n, w.s_ntt, &te);
+        b.t = ntt_tables_get(device_, fr_of(j.omega_ext), (int)j.log_ext, w.s_ntt, &te);
+        b.pre = pow_tables_get(device_, fr_of(j.coset), (int)j.log_ext, w.s_ntt, &te);
+        if (!a.t || !b.t || !b.pre) {
+          ok(te == cudaSuccess ? cudaErrorInvalidValue : te);
+          break;
+        }
+        a.data = d;  // ifft in place on the first n slots of the extended buffer
+        a.tmp = tmp;
+        a.has_post = true;
+        a.post = fr_of(j.scale);
+        a.level0 = 0;
+        a.dep_job = -1;
+        b.data = d;
+        b.tmp = tmp;
+        b.has_post = false;
+        b.level0 = a.t->plan.npass;
+        b.dep_job = (int)items.size();
+        items.push_back(a);
+        items.push_back(b);
+      }
+      ntt_outputs.push_back({r, d});
+    }
+    if (e == cudaSuccess && !items.empty()) {
+      // level-ordered work list over all transforms of the wave
+      int max_level = 0;
+      for (auto& it : items) max_level = std::max(max_level, it.level0 + it.t->plan.npass);
+      std::vector<int> last_pass(items.size(), -1);
+      uint64_t tiles = 0;
+      for (int lvl = 0; lvl < max_level; lvl++) {
+        for (size_t i = 0; i < items.size(); i++) {
+          const NttItem& it = items[i];
+          const int k = lvl - it.level0;
+          if (k < 0 || k >= it.t->plan.npass) continue;
+          BatchPass bp{};
+          const uint64_t ncta =
+              ntt_pass_params(*it.t, k, it.data, it.tmp, it.pre, it.has_post ? &it.post : nullptr, &bp.p);
+          bp.B = (uint32_t)it.t->plan.bits[k];
+          bp.ntiles = (uint32_t)ncta;
+          bp.tile_base = (uint32_t)tiles;
+          int dep = k > 0 ? last_pass[i] : (it.dep_job >= 0 ? last_pass[it.dep_job] : -1);
+          bp.dep = dep < 0 ? ~0u : (uint32_t)dep;
+          bp.dep_tiles = dep < 0 ? 0u : w.passes[dep].ntiles;
+          last_pass[i] = (int)w.passes.size();
+          w.passes.push_back(bp);
+          tiles += ncta;
+        }
+      }
+      BatchPass* dp = nullptr;
+      uint32_t* dc = nullptr;
+      const size_t np = w.passes.size();
+      if (ok(cudaMallocAsync((void**)&dp, np * sizeof(BatchPass), w.s_ntt)) &&
+          ok(cudaMallocAsync((void**)&dc, (2 + np) * 4, w.s_ntt)) &&
+          ok(cudaMemcpyAsync(dp, w.passes.data(), np * sizeof(BatchPass), cudaMemcpyHostToDevice, w.s_ntt)) &&
+          ok(cudaMemsetAsync(dc, 0, (2 + np) * 4, w.s_ntt))) {
+        ok(ntt_batch_launch(dp, (uint32_t)np, (uint32_t)tiles, dc, dc + 2, dc + 1, grid_, w.s_ntt));
+        ok(cudaMemcpyAsync(w.mailbox, dc + 1, 4, cudaMemcpyDeviceToHost, w.s_ntt));
+        batch_launches_++;
+      }
+      frees_ntt.push_back(dp);
+      frees_ntt.push_back(dc);
+      for (auto& o : ntt_outputs) {
+        const zkgpu_job& j = o.first->job;
+        const uint32_t L = j.kind == ZKGPU_KIND_LDE ? j.log_ext : j.log_n;
+        ok(cudaMemcpyAsync(j.output, o.second, ((size_t)1 << L) * 32, cudaMemcpyDeviceToHost, w.s_ntt));
+      }
+    }
+    for (void* p : frees_ntt)
+      if (p) cudaFreeAsync(p, w.s_ntt);
+    for (void* p : frees_msm)
+      if (p) cudaFreeAsync(p, w.s_msm);
+    cudaEventRecord(w.ev_ntt, w.s_ntt);
+    cudaEventRecord(w.ev_msm, w.s_msm);
+    if (e != cudaSuccess) w.status = status_of("server wave", e);
+  }
+
+  void comp_loop() {
+    cudaSetDevice(device_);
+    for (;;) {
+      std::unique_ptr<Wave> w;
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_comp_.wait(lk, [&] { return !inflight_.empty() || (stop_ && inflight_.empty()); });
+        if (inflight_.empty()) return;
+        w = std::move(inflight_.front());
+        inflight_.pop_front();
+      }
+      cudaError_t e1 = cudaEventSynchronize(w->ev_ntt);
+      cudaError_t e2 = cudaEventSynchronize(w->ev_msm);
+      int st = w->status;
+      if (st == ZKGPU_OK && (e1 != cudaSuccess || e2 != cudaSuccess))
+        st = status_of("server wave sync", e1 != cudaSuccess ? e1 : e2);
+      if (st == ZKGPU_OK && (uint32_t)w->mailbox[0]) st = ZKGPU_ETIMEOUT;
+      const auto now = clk::now();
+      for (JobRec* r : w->jobs)
+        if (st == ZKGPU_OK && r->job.kind == ZKGPU_KIND_MSM && r->msm_out) {
+          host::fq::normalize_jacobian(r->msm_out);
+          std::memcpy(r->job.output, r->msm_out, 96);
+        }
+      cudaEventDestroy(w->ev_ntt);
+      cudaEventDestroy(w->ev_msm);
+      {
+        std::lock_guard<std::mutex> lk(mu_);
+        for (JobRec* r : w->jobs) {
+          r->status = st;
+          r->t_done = now;
+          adm_.release(r->bytes);
+          if (st == ZKGPU_OK)
+            completed_++;
+          else
+            failed_++;
+        }
+        inflight_jobs_ -= w->jobs.size();
+        waves_inflight_--;
+        retired_gen_++;
+      }
+      cv_done_.notify_all();
+      cv_sched_.notify_all();
+    }
+  }
+
+  int device_;
+  AdmissionQueue adm_;
+  uint32_t max_wave_;
+  int grid_ = 0;
+  cudaStream_t s_ntt_[kStreams] = {}, s_msm_[kStreams] = {};
+  std::mutex mu_;
+  std::condition_variable cv_sched_, cv_comp_, cv_done_;
+  std::unordered_map<uint64_t, std::unique_ptr<JobRec>> jobs_;
+  std::deque<std::unique_ptr<Wave>> inflight_;
+  std::vector<BaseSet> bases_;
+  std::thread sched_, comp_;
+  bool stop_ = false;
+  uint64_t next_ticket_ = 1, submitted_ = 0, rejected_ = 0, completed_ = 0, failed_ = 0, waves_ = 0;
+  uint64_t batch_launches_ = 0, peak_ = 0, inflight_jobs_ = 0, retired_gen_ = 0;
+  int waves_inflight_ = 0;
+  uint64_t* mailbox_ = nullptr;
+  uint64_t slot_words_ = 0;
+};
+
+}  // namespace zk
+
+extern "C" uint64_t zkgpu_job_footprint(const zkgpu_job* j) {
+  if (!j) return 0;
+  switch (j->kind) {
+    case ZKGPU_KIND_NTT:
+      return 2 * ((uint64_t)1 << j->log_n) * 32 + 4096;
+    case ZKGPU_KIND_LDE:
+      return 2 * ((uint64_t)1 << j->log_ext) * 32 + 4096;
+    case ZKGPU_KIND_MSM:
+      return j->n * 32 + zk::msm_scratch_bytes(j->n);
+    default:
+      return 0;
+  }
+}
+
+extern "C" uint64_t zkgpu_admission_simulate(uint64_t budget, const uint64_t* fp, uint32_t n, int32_t* rounds) {
+  zk::AdmissionQueue q(budget);
+  for (uint32_t i = 0; i < n; i++) {
+    if (!q.push(i, fp[i])) rounds[i] = -1;
+  }
+  uint64_t peak = 0;
+  int32_t round = 0;
+  while (q.pending()) {
+    std::vector<uint64_t> adm = q.admit();
+    peak = std::max(peak, q.used());
+    for (uint64_t t : adm) rounds[t] = round;
+    for (uint64_t t : adm) q.release(fp[t]);  // each admitted job finishes this round
+    round++;
+  }
+  return peak;
+}
+
+extern "C" int zkgpu_server_create(int device, uint64_t hbm_budget_bytes, uint32_t max_wave_jobs, void** server) {
+  if (!server) return ZKGPU_EINVAL;
+  cudaStream_t s;
+  int st = zk::bind_device(device, &s);
+  if (st) return st;
+  auto srv = std::make_unique<zk::Server>(device, hbm_budget_bytes, max_wave_jobs);
+  st = srv->start();
+  if (st) return st;
+  *server = srv.release();
+  return ZKGPU_OK;
+}
+
+extern "C" int zkgpu_server_add_bases(void* server, const uint64_t* xy, uint64_t n, uint32_t* id) {
+  if (!server || !id || (n && !xy)) return ZKGPU_EINVAL;
+  return static_cast<zk::Server*>(server)->add_bases(xy, n, id);
+}
+
+extern "C" int zkgpu_server_submit(void* server, const zkgpu_job* job, uint64_t* ticket) {
+  if (!server || !job || !ticket || !job->output) return ZKGPU_EINVAL;
+  if (job->kind == ZKGPU_KIND_NTT || job->kind == ZKGPU_KIND_LDE) {
+    if (!job->input || job->log_n < 3 || job->log_n > (uint32_t)zk::NTT_MAX_LOG) return ZKGPU_EINVAL;
+    zk::host::Fr w = zk::fr_of(job->omega);
+    if (!zk::host::is_canonical(w) || !zk::host::is_primitive_root(w, job->log_n)) return ZKGPU_EINVAL;
+    if (job->kind == ZKGPU_KIND_LDE) {
+      zk::host::Fr we = zk::fr_of(job->omega_ext);
+      if (job->log_ext < job->log_n || job->log_ext > (uint32_t)zk::NTT_MAX_LOG || !zk::host::is_canonical(we) ||
+          !zk::host::is_primitive_root(we, job->log_ext))
+        return ZKGPU_EINVAL;
+    }
+  } else if (job->kind == ZKGPU_KIND_MSM) {
+    if ((job->n && !job->input) || job->n >= (1ull << 31)) return ZKGPU_EINVAL;
+  } else {
+    return ZKGPU_EINVAL;
+  }
+  return static_cast<zk::Server*>(server)->submit(job, ticket);
+}
+
+extern "C" int zkgpu_server_wait(void* server, uint64_t ticket, uint32_t timeout_ms, double* latency_ms) {
+  if (!server) return ZKGPU_EINVAL;
+  return static_cast<zk::Server*>(server)->wait(ticket, timeout_ms, latency_ms);
+}
+
+extern "C" int zkgpu_server_stats_get(void* server, zkgpu_server_stats* out) {
+  if (!server || !out) return ZKGPU_EINVAL;
+  static_cast<zk::Server*>(server)->stats(out);
+  return ZKGPU_OK;
+}
+
+extern "C" void zkgpu_server_destroy(void* server) { delete static_cast<zk::Server*>(server); }
