@@ -462,7 +462,7 @@ def serving_trace(njobs: int, rate: float, seed: int = 99):
     return out
 
 
-def bench_serving(zk, torch, dev: int, njobs: int = 1000, rate: float = 2000.0):
+def bench_serving(zk, torch, dev: int, njobs: int = 1000, rate: float = 2000.0, wave_jobs: int = 32):
     """Serving loop (continuous batching) vs one call per job on the same GPU,
     same arrival trace; host buffers pinned, shared per size class (read-only
     inputs; outputs of identical jobs are identical)."""
@@ -508,7 +508,7 @@ def bench_serving(zk, torch, dev: int, njobs: int = 1000, rate: float = 2000.0):
         return float(np.percentile(np.asarray(x), q)) if len(x) else None
 
     # ---- serving loop ----
-    srv = zk.Server(device=dev, hbm_budget=150 * 10**9)
+    srv = zk.Server(device=dev, hbm_budget=150 * 10**9, max_wave_jobs=wave_jobs)
     bid = srv.add_bases(bases)
 
     def run_server(open_loop: bool):

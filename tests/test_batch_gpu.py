@@ -46,8 +46,11 @@ def test_batch_uneven_sizes_two_runs(zk, oracle):
     for j, ref in zip(jobs, refs):
         assert np.array_equal(j["tensor"].cpu().numpy().view(np.uint64), ref), j["log_n"]
     # second run: refill the same buffers with new inputs; the graph is replayed
-    rng2 = np.random.default_rng(5)  # same sizes / flags, new data seeds
+    rng2 = np.random.default_rng(5)  # replay the same draws: sizes, then per-job flags
+    rng2.integers(3, 18, 48)
     jobs2, refs2 = make_jobs(oracle, torch, rng2, sizes, 900)
+    for j, j2 in zip(jobs, jobs2):
+        assert ("coset" in j) == ("coset" in j2) and ("scale" in j) == ("scale" in j2)
     for j, j2 in zip(jobs, jobs2):
         j["tensor"].copy_(j2["tensor"])
     batch.run()

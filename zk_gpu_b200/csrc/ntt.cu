@@ -316,6 +316,7 @@ __global__ void __launch_bounds__(256, 2) ntt_batch_kernel(const BatchPass* pass
       case 11: ntt_pass_tile<11, true>(bp.p, tile, smem); break;
       default: break;
     }
+    __threadfence();  // every thread publishes its own stores before the tile is counted
     __syncthreads();
     if (threadIdx.x == 0) {
       __threadfence();
