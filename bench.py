@@ -98,6 +98,7 @@ class ClockSampler:
         self.gpu = gpu_index
         self.proc = None
         self.lines: list[str] = []
+        self.stamped: list = []  # (perf_counter, csv line)
 
     def __enter__(self):
         try:
@@ -106,13 +107,23 @@ class ClockSampler:
                  "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self._t = threading.Thread(target=self._read, daemon=True)
             self._t.start()
+            # nvidia-smi's start-up (NVML init) disturbs a running GPU context:
+            # let it settle before anything is timed
+            deadline = time.perf_counter() + 5.0
+            while not self.stamped and time.perf_counter() < deadline:
+                time.sleep(0.02)
         except (OSError, FileNotFoundError):
             self.proc = None
         return self
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.stamped.append((time.perf_counter(), line.strip()))
+
+    def window(self, t0: float, t1: float):
+        """keep only samples taken inside [t0, t1] (the timed region)"""
+        inside = [ln for (t, ln) in self.stamped if t0 <= t <= t1]
+        self.lines = inside if inside else [ln for (_, ln) in self.stamped[-3:]]
 
     def __exit__(self, *exc):
         if self.proc:
@@ -238,24 +249,27 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         zk.lagrange_to_extended_dev(d_vals, d_ext, LOG_N, LOG_EXT, c["omega_inv"], c["divisor"], c["g"],
                                     c["omega_ext"], stream=stream)
 
-    with torch.cuda.stream(stream):
-        for _ in range(max(args.warmup, 3)):
-            step()
-    stream.synchronize()
-
-    # ---- timed region: device-resident pipeline ----
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    zk.prof_reset()
-    zk.prof_enable(True)
-    zk.launch_count(reset=True)
-    barrier()
-    torch.cuda.synchronize()
     with ClockSampler(dev) as clk:
+        with torch.cuda.stream(stream):
+            for _ in range(max(args.warmup, 3)):
+                step()
+        stream.synchronize()
+
+        # ---- timed region: device-resident pipeline ----
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        zk.prof_reset()
+        zk.prof_enable(True)
+        zk.launch_count(reset=True)
+        barrier()
+        torch.cuda.synchronize()
+        t_begin = time.perf_counter()
         e0.record(stream)
         for _ in range(args.steps):
             step()
         e1.record(stream)
         stream.synchronize()
+        t_end = time.perf_counter()
+    clk.window(t_begin, t_end)
     torch.cuda.synchronize()
     barrier()
     launches = zk.launch_count()

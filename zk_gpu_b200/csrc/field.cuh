@@ -407,13 +407,54 @@ __device__ __forceinline__ void mul29_limbs(uint32_t rl[9], const uint32_t al[9]
   rl[8] = (uint32_t)c;
 }
 
+// Same product in column (product-scanning) order: column k collects
+// a_j b_(k-j) and m_j p_(k-j) in one 64-bit accumulator (< 18 * 2^58 + 2^35),
+// so only that accumulator and the 9 quotient digits m_j stay live
+// (register-light; measured a little faster than the row order).
+template <class P>
+__device__ __forceinline__ void mul29_cols(uint32_t rl[9], const uint32_t al[9], const uint32_t bl[9]) {
+  uint32_t m[9];
+  uint64_t acc = 0;
+#pragma unroll
+  for (int k = 0; k < 17; k++) {
+#pragma unroll
+    for (int j = 0; j < 9; j++) {
+      const int i = k - j;
+      if (i >= 0 && i < 9) acc += (uint64_t)al[j] * bl[i];
+    }
+#pragma unroll
+    for (int j = 0; j < 9; j++) {
+      const int i = k - j;
+      if (j < k && i >= 0 && i < 9) acc += (uint64_t)m[j] * p29<P>(i);
+    }
+    if (k < 9) {
+      m[k] = ((uint32_t)acc * inv29<P>()) & M29;
+      acc += (uint64_t)m[k] * p29<P>(0);
+      acc >>= 29;  // low 29 bits are zero
+    } else {
+      rl[k - 9] = (uint32_t)acc & M29;
+      acc >>= 29;
+    }
+  }
+  rl[8] = (uint32_t)acc;
+}
+
+// a (8 words, R form) times a pre-split R'-form constant b (9 limbs)
+template <class P>
+__device__ __forceinline__ void mul_r29_pre(uint32_t r[8], const uint32_t a[8], const uint32_t bl[9]) {
+  uint32_t al[9], rl[9];
+  split29(al, a);
+  mul29_cols<P>(rl, al, bl);
+  pack29(r, rl);
+}
+
 // 8-word interface: r = a * b' * 2^-261 (b' in R' form), lazy (< 2p).
 template <class P>
 __device__ __forceinline__ void mul_r29(uint32_t r[8], const uint32_t a[8], const uint32_t b[8]) {
   uint32_t al[9], bl[9], rl[9];
   split29(al, a);
   split29(bl, b);
-  mul29_limbs<P>(rl, al, bl);
+  mul29_cols<P>(rl, al, bl);
   pack29(r, rl);
 }
 

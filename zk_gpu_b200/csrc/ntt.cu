@@ -61,6 +61,11 @@ __device__ __forceinline__ void ld_smem_fe(uint32_t r[8], const uint32_t* plane0
 #pragma unroll
   for (int k = 0; k < 8; k++) r[k] = plane0[k * plane_stride + a];
 }
+// a twiddle stored as 9 pre-split 29-bit limb planes
+__device__ __forceinline__ void ld_smem_tw(uint32_t r[9], const uint32_t* plane0, uint32_t plane_stride, uint32_t a) {
+#pragma unroll
+  for (int k = 0; k < 9; k++) r[k] = plane0[k * plane_stride + a];
+}
 __device__ __forceinline__ void st_smem_fe(uint32_t* plane0, uint32_t plane_stride, uint32_t a, const uint32_t r[8]) {
 #pragma unroll
   for (int k = 0; k < 8; k++) plane0[k * plane_stride + a] = r[k];
@@ -88,15 +93,15 @@ __device__ __forceinline__ void ntt_round(uint32_t x[8][8], uint32_t q, const ui
 #pragma unroll
           for (int k = 0; k < 8; k++) x[r2][k] = t[k];
         } else {
-          uint32_t w[8];
-          ld_smem_fe(w, tws, HALF, e);
-          mul_r29<P_r>(x[r2], t, w);
+          uint32_t w[9];
+          ld_smem_tw(w, tws, HALF, e);
+          mul_r29_pre<P_r>(x[r2], t, w);
         }
       } else {
         const uint32_t e = ((q & ((1u << LO) - 1u)) | ((uint32_t)(r & ((1 << rb) - 1)) << LO)) << (B - 1 - b);
-        uint32_t w[8];
-        ld_smem_fe(w, tws, HALF, e);
-        mul_r29<P_r>(x[r2], t, w);
+        uint32_t w[9];
+        ld_smem_tw(w, tws, HALF, e);
+        mul_r29_pre<P_r>(x[r2], t, w);
       }
     }
   }
@@ -151,9 +156,11 @@ __device__ __forceinline__ void ntt_pass_tile(const PassParams& p, uint64_t tile
   const bool active = !BATCH || g < G;
 
   for (uint32_t e = tid; e < M / 2; e += blockDim.x) {
-    uint32_t w[8];
+    uint32_t w[8], wl[9];
     ld_fe_nc(w, p.inner + e);
-    st_smem_fe(tws, M / 2, e, w);
+    split29(wl, w);  // stored pre-split: 9 limb planes
+#pragma unroll
+    for (int k = 0; k < 9; k++) tws[k * (M / 2) + e] = wl[k];
   }
 
   const uint64_t J = 1ull << p.log_J;
@@ -581,7 +588,7 @@ template <int B>
 static cudaError_t launch_pass(const PassParams& pp, uint64_t ncta, cudaStream_t s) {
   constexpr uint32_t M = 1u << B;
   const uint32_t threads = pp.G * (M / 8);
-  const size_t smem = (size_t)8 * pp.G * M * 4 + (size_t)(M / 2) * 32;
+  const size_t smem = (size_t)8 * pp.G * M * 4 + (size_t)(M / 2) * 36;
   static bool attr_set[64] = {false};
   int dev = 0;
   cudaGetDevice(&dev);
@@ -689,7 +696,7 @@ cudaError_t ntt_run(const NttTables& t, fe* d_a, fe* d_tmp, const PowTables* pre
   return cudaSuccess;
 }
 
-static size_t batch_smem_bytes() { return (size_t)8 * 2048 * 4 + (size_t)1024 * 32; }  // B <= 11
+static size_t batch_smem_bytes() { return (size_t)8 * 2048 * 4 + (size_t)1024 * 36; }  // B <= 11
 
 int ntt_batch_grid(int device) {
   static int cached[64] = {0};
