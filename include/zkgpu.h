@@ -214,6 +214,11 @@ void zkgpu_server_destroy(void *server);
 /* elementwise field op on host arrays through the device kernels:
  * op 0 = mul, 1 = add, 2 = sub;  fid 0 = Fr, 1 = Fq */
 int zkgpu_field_op(int device, int op, int fid, const uint64_t *a, const uint64_t *b, uint64_t *out, uint64_t n);
+/* failure detection: runs a batch whose dependency wait can never be met;
+ * the kernel gives up after about spin_us and the call returns
+ * ZKGPU_ETIMEOUT (omega12: a root of order 2^12).  No counterpart in the
+ * reference, whose scheduler waits without limit (src/gpulock.rs:191-194). */
+int zkgpu_selftest_wait_timeout(int device, const uint64_t omega12[4], uint32_t spin_us);
 /* message of the last ZKGPU_ECUDA on this thread ("" if none) */
 const char *zkgpu_last_error(void);
 /* kernel launches issued by this thread since the last reset */

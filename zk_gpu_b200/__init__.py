@@ -71,6 +71,7 @@ EXPORTS = {
     "zkgpu_ntt_batch_check": (_i32, [P]),
     "zkgpu_ntt_batch_info": (None, [P, P, P, P]),
     "zkgpu_ntt_batch_destroy": (None, [P]),
+    "zkgpu_selftest_wait_timeout": (_i32, [_i32, P, _u32]),
     "zkgpu_job_footprint": (_u64, [P]),
     "zkgpu_admission_simulate": (_u64, [_u64, P, _u32, P]),
     "zkgpu_server_create": (_i32, [_i32, _u64, _u32, P]),

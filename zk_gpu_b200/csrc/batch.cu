@@ -201,6 +201,57 @@ extern "C" void zkgpu_ntt_batch_info(void* handle, uint32_t* passes, uint32_t* t
   if (grid) *grid = b->grid;
 }
 
+// Failure detection without a fault: a two-pass transform whose second pass
+// waits for one tile more than the first pass has, so nothing ever satisfies
+// the wait.  The kernel must give up after ~spin_us, record the error and
+// return; the call reports ZKGPU_ETIMEOUT and the context stays usable.
+extern "C" int zkgpu_selftest_wait_timeout(int device, const uint64_t omega12[4], uint32_t spin_us) {
+  if (!omega12 || spin_us == 0 || spin_us > 2000000) return ZKGPU_EINVAL;
+  cudaStream_t s;
+  int st = zk::bind_device(device, &s);
+  if (st) return st;
+  const int L = 12;
+  hf::Fr w = fr_of(omega12);
+  if (!hf::is_canonical(w) || !hf::is_primitive_root(w, L)) return ZKGPU_EINVAL;
+  cudaError_t e;
+  const zk::NttTables* t = zk::ntt_tables_get(device, w, L, s, &e);
+  if (!t) return zk::status_of("ntt_tables_get", e);
+  if (t->plan.npass != 2) return ZKGPU_EINVAL;
+  fe *d = nullptr, *tmp = nullptr;
+  zk::BatchPass* dp = nullptr;
+  uint32_t* dc = nullptr;
+  ZK_TRY("cudaMalloc", cudaMalloc((void**)&d, (2u << L) * sizeof(fe)));
+  tmp = d + (1u << L);
+  zk::BatchPass bp[2] = {};
+  uint64_t tiles = 0;
+  for (int k = 0; k < 2; k++) {
+    bp[k].ntiles = (uint32_t)zk::ntt_pass_params(*t, k, d, tmp, nullptr, nullptr, &bp[k].p);
+    bp[k].B = (uint32_t)t->plan.bits[k];
+    bp[k].tile_base = (uint32_t)tiles;
+    tiles += bp[k].ntiles;
+  }
+  bp[0].dep = ~0u;
+  bp[1].dep = 0;
+  bp[1].dep_tiles = bp[0].ntiles + 1;  // never reached
+  int ds;
+  cudaDeviceGetAttribute(&ds, cudaDevAttrClockRate, device);  // kHz
+  const uint64_t spin = (uint64_t)spin_us * (uint64_t)(ds > 0 ? ds : 2000000) / 1000ull;
+  e = cudaMemset(d, 0, (2u << L) * sizeof(fe));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&dp, sizeof(bp));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&dc, 4 * 4);
+  if (e == cudaSuccess) e = cudaMemcpy(dp, bp, sizeof(bp), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(dc, 0, 4 * 4);
+  if (e == cudaSuccess) e = zk::ntt_batch_launch(dp, 2, (uint32_t)tiles, dc, dc + 2, dc + 1, zk::ntt_batch_grid(device), s, spin);
+  uint32_t err = 0;
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = cudaMemcpy(&err, dc + 1, 4, cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (dp) cudaFree(dp);
+  if (dc) cudaFree(dc);
+  if (e != cudaSuccess) return zk::status_of("selftest_wait_timeout", e);
+  return err ? ZKGPU_ETIMEOUT : ZKGPU_OK;
+}
+
 extern "C" void zkgpu_ntt_batch_destroy(void* handle) {
   auto* b = static_cast<zk::NttBatch*>(handle);
   if (!b) return;

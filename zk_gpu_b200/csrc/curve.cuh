@@ -7,8 +7,13 @@
 // P == -Q -> identity) handled explicitly, which the reference's Jacobian
 // code gets wrong (cuda/curve.cuh:13-20, 170-179: its "identity" (0,0,R) is
 // not recognised as zero afterwards).  Affine inputs use (0, 0) for the
-// identity (cuda/bn256.h:15-20).  All arithmetic is canonical (values < q)
-// because the equality tests need canonical representatives.
+// identity (cuda/bn256.h:15-20).
+//
+// Arithmetic form: every coordinate is kept in the R' = 2^261 Montgomery
+// form of the radix-2^29 product (mul_r29: R'-form x R'-form -> R'-form),
+// lazily reduced in [0, 2q); values are made canonical only where they are
+// compared with zero.  to_rprime / from_rprime convert from / to the
+// R = 2^256 form used in memory by the API (bit-identical to halo2curves).
 #pragma once
 #include "field.cuh"
 
@@ -23,13 +28,39 @@ struct aff_t {
   uint32_t x[8], y[8];
 };
 
+// ---- lazy R'-form Fq helpers --------------------------------------------
+__device__ __forceinline__ void qmul(uint32_t r[8], const uint32_t a[8], const uint32_t b[8]) { mul_r29<P_q>(r, a, b); }
+__device__ __forceinline__ void qsqr(uint32_t r[8], const uint32_t a[8]) { mul_r29<P_q>(r, a, a); }
+__device__ __forceinline__ void qadd(uint32_t r[8], const uint32_t a[8], const uint32_t b[8]) { add_lazy<P_q>(r, a, b); }
+__device__ __forceinline__ void qsub(uint32_t r[8], const uint32_t a[8], const uint32_t b[8]) { sub_lazy<P_q>(r, a, b); }
+__device__ __forceinline__ void qdbl(uint32_t r[8], const uint32_t a[8]) { add_lazy<P_q>(r, a, a); }
+__device__ __forceinline__ bool qzero(const uint32_t a[8]) {
+  uint32_t c[8];
+  reduce_once<P_q>(c, a);
+  return is_zero(c);
+}
+// x (R form, x * 2^256) -> x * 2^261, canonical: multiply by 2^266 mod q
+__device__ __forceinline__ void to_rprime(uint32_t r[8], const uint32_t a[8]) {
+  const uint32_t k[8] = {0x13349ca1u, 0xb34bb095u, 0xf028f972u, 0x1e880124u,
+                         0xa6092b95u, 0xe56cdd25u, 0xdce9ed32u, 0x05800320u};
+  mul_r29<P_q>(r, a, k);
+  reduce_once<P_q>(r, r);
+}
+// x * 2^261 (lazy) -> x * 2^256, canonical: multiply by 2^256 mod q
+__device__ __forceinline__ void from_rprime(uint32_t r[8], const uint32_t a[8]) {
+  uint32_t one_r[8];
+  set_one<P_q>(one_r);  // the integer 2^256 mod q
+  mul_r29<P_q>(r, a, one_r);
+  reduce_once<P_q>(r, r);
+}
+
 __device__ __forceinline__ void xyzz_set_inf(xyzz_t& p) {
   set_zero(p.x);
   set_zero(p.y);
   set_zero(p.zz);
   set_zero(p.zzz);
 }
-__device__ __forceinline__ bool xyzz_is_inf(const xyzz_t& p) { return is_zero(p.zz); }
+__device__ __forceinline__ bool xyzz_is_inf(const xyzz_t& p) { return qzero(p.zz); }
 __device__ __forceinline__ bool aff_is_inf(const aff_t& p) { return is_zero(p.x) && is_zero(p.y); }
 
 __device__ __forceinline__ void xyzz_from_aff(xyzz_t& r, const aff_t& q) {
@@ -39,30 +70,30 @@ __device__ __forceinline__ void xyzz_from_aff(xyzz_t& r, const aff_t& q) {
   }
   cpy(r.x, q.x);
   cpy(r.y, q.y);
-  set_one<P_q>(r.zz);
-  set_one<P_q>(r.zzz);
+  set_one_r29<P_q>(r.zz);
+  set_one_r29<P_q>(r.zzz);
 }
 
 // r = 2p  (dbl-2008-s-1, a = 0).  The identity doubles to itself (ZZ stays 0).
 __device__ __forceinline__ void xyzz_dbl(xyzz_t& r, const xyzz_t& p) {
   uint32_t U[8], V[8], W[8], S[8], M[8], t[8];
-  dbl<P_q>(U, p.y);
-  sqr<P_q>(V, U);
-  mul<P_q>(W, U, V);
-  mul<P_q>(S, p.x, V);
-  sqr<P_q>(M, p.x);
-  dbl<P_q>(t, M);
-  add<P_q>(M, M, t);  // M = 3 X^2
+  qdbl(U, p.y);
+  qsqr(V, U);
+  qmul(W, U, V);
+  qmul(S, p.x, V);
+  qsqr(M, p.x);
+  qdbl(t, M);
+  qadd(M, M, t);  // M = 3 X^2
   uint32_t X3[8], Y3[8];
-  sqr<P_q>(X3, M);
-  dbl<P_q>(t, S);
-  sub<P_q>(X3, X3, t);
-  sub<P_q>(t, S, X3);
-  mul<P_q>(Y3, M, t);
-  mul<P_q>(t, W, p.y);
-  sub<P_q>(Y3, Y3, t);
-  mul<P_q>(r.zz, V, p.zz);
-  mul<P_q>(r.zzz, W, p.zzz);
+  qsqr(X3, M);
+  qdbl(t, S);
+  qsub(X3, X3, t);
+  qsub(t, S, X3);
+  qmul(Y3, M, t);
+  qmul(t, W, p.y);
+  qsub(Y3, Y3, t);
+  qmul(r.zz, V, p.zz);
+  qmul(r.zzz, W, p.zzz);
   cpy(r.x, X3);
   cpy(r.y, Y3);
 }
@@ -74,20 +105,20 @@ __device__ __forceinline__ void xyzz_mdbl(xyzz_t& r, const aff_t& q) {
     return;
   }
   uint32_t U[8], V[8], W[8], S[8], M[8], t[8];
-  dbl<P_q>(U, q.y);
-  sqr<P_q>(V, U);
-  mul<P_q>(W, U, V);
-  mul<P_q>(S, q.x, V);
-  sqr<P_q>(M, q.x);
-  dbl<P_q>(t, M);
-  add<P_q>(M, M, t);
-  sqr<P_q>(r.x, M);
-  dbl<P_q>(t, S);
-  sub<P_q>(r.x, r.x, t);
-  sub<P_q>(t, S, r.x);
-  mul<P_q>(r.y, M, t);
-  mul<P_q>(t, W, q.y);
-  sub<P_q>(r.y, r.y, t);
+  qdbl(U, q.y);
+  qsqr(V, U);
+  qmul(W, U, V);
+  qmul(S, q.x, V);
+  qsqr(M, q.x);
+  qdbl(t, M);
+  qadd(M, M, t);
+  qsqr(r.x, M);
+  qdbl(t, S);
+  qsub(r.x, r.x, t);
+  qsub(t, S, r.x);
+  qmul(r.y, M, t);
+  qmul(t, W, q.y);
+  qsub(r.y, r.y, t);
   cpy(r.zz, V);
   cpy(r.zzz, W);
 }
@@ -100,34 +131,34 @@ __device__ __forceinline__ void xyzz_madd(xyzz_t& p, const aff_t& q) {
     return;
   }
   uint32_t U2[8], S2[8], P[8], R[8];
-  mul<P_q>(U2, q.x, p.zz);
-  mul<P_q>(S2, q.y, p.zzz);
-  sub<P_q>(P, U2, p.x);
-  sub<P_q>(R, S2, p.y);
-  if (is_zero(P)) {
-    if (is_zero(R))
+  qmul(U2, q.x, p.zz);
+  qmul(S2, q.y, p.zzz);
+  qsub(P, U2, p.x);
+  qsub(R, S2, p.y);
+  if (qzero(P)) {
+    if (qzero(R))
       xyzz_mdbl(p, q);
     else
       xyzz_set_inf(p);
     return;
   }
   uint32_t PP[8], PPP[8], Q[8], t[8];
-  sqr<P_q>(PP, P);
-  mul<P_q>(PPP, P, PP);
-  mul<P_q>(Q, p.x, PP);
-  sqr<P_q>(t, R);
-  sub<P_q>(t, t, PPP);
+  qsqr(PP, P);
+  qmul(PPP, P, PP);
+  qmul(Q, p.x, PP);
+  qsqr(t, R);
+  qsub(t, t, PPP);
   uint32_t X3[8];
-  dbl<P_q>(X3, Q);
-  sub<P_q>(X3, t, X3);
-  sub<P_q>(t, Q, X3);
-  mul<P_q>(t, R, t);
+  qdbl(X3, Q);
+  qsub(X3, t, X3);
+  qsub(t, Q, X3);
+  qmul(t, R, t);
   uint32_t u[8];
-  mul<P_q>(u, p.y, PPP);
-  sub<P_q>(p.y, t, u);
+  qmul(u, p.y, PPP);
+  qsub(p.y, t, u);
   cpy(p.x, X3);
-  mul<P_q>(p.zz, p.zz, PP);
-  mul<P_q>(p.zzz, p.zzz, PPP);
+  qmul(p.zz, p.zz, PP);
+  qmul(p.zzz, p.zzz, PPP);
 }
 
 // p += q (both XYZZ), add-2008-s with all special cases
@@ -138,36 +169,36 @@ __device__ __forceinline__ void xyzz_add(xyzz_t& p, const xyzz_t& q) {
     return;
   }
   uint32_t U1[8], U2[8], S1[8], S2[8], P[8], R[8];
-  mul<P_q>(U1, p.x, q.zz);
-  mul<P_q>(U2, q.x, p.zz);
-  mul<P_q>(S1, p.y, q.zzz);
-  mul<P_q>(S2, q.y, p.zzz);
-  sub<P_q>(P, U2, U1);
-  sub<P_q>(R, S2, S1);
-  if (is_zero(P)) {
-    if (is_zero(R))
+  qmul(U1, p.x, q.zz);
+  qmul(U2, q.x, p.zz);
+  qmul(S1, p.y, q.zzz);
+  qmul(S2, q.y, p.zzz);
+  qsub(P, U2, U1);
+  qsub(R, S2, S1);
+  if (qzero(P)) {
+    if (qzero(R))
       xyzz_dbl(p, p);
     else
       xyzz_set_inf(p);
     return;
   }
   uint32_t PP[8], PPP[8], Q[8], t[8], X3[8];
-  sqr<P_q>(PP, P);
-  mul<P_q>(PPP, P, PP);
-  mul<P_q>(Q, U1, PP);
-  sqr<P_q>(t, R);
-  sub<P_q>(t, t, PPP);
-  dbl<P_q>(X3, Q);
-  sub<P_q>(X3, t, X3);
-  sub<P_q>(t, Q, X3);
-  mul<P_q>(t, R, t);
-  mul<P_q>(S1, S1, PPP);
-  sub<P_q>(p.y, t, S1);
+  qsqr(PP, P);
+  qmul(PPP, P, PP);
+  qmul(Q, U1, PP);
+  qsqr(t, R);
+  qsub(t, t, PPP);
+  qdbl(X3, Q);
+  qsub(X3, t, X3);
+  qsub(t, Q, X3);
+  qmul(t, R, t);
+  qmul(S1, S1, PPP);
+  qsub(p.y, t, S1);
   cpy(p.x, X3);
-  mul<P_q>(p.zz, p.zz, q.zz);
-  mul<P_q>(p.zz, p.zz, PP);
-  mul<P_q>(p.zzz, p.zzz, q.zzz);
-  mul<P_q>(p.zzz, p.zzz, PPP);
+  qmul(p.zz, p.zz, q.zz);
+  qmul(p.zz, p.zz, PP);
+  qmul(p.zzz, p.zzz, q.zzz);
+  qmul(p.zzz, p.zzz, PPP);
 }
 
 // p = k * p for a small non-negative k (double-and-add, k < 2^32)
@@ -187,19 +218,22 @@ __device__ __forceinline__ void xyzz_mul_small(xyzz_t& p, uint32_t k) {
   p = acc;
 }
 
-// XYZZ -> Jacobian without inversion: (X ZZ^2, Y ZZ^3, ZZZ)
+// XYZZ (R' form) -> Jacobian (R form, canonical) without inversion:
+// (X ZZ^2, Y ZZ^3, ZZZ) represents the same point.
 __device__ __forceinline__ void xyzz_to_jacobian(uint32_t out[24], const xyzz_t& p) {
   if (xyzz_is_inf(p)) {
 #pragma unroll
     for (int i = 0; i < 24; i++) out[i] = 0;
     return;
   }
-  uint32_t zz2[8], zz3[8];
-  sqr<P_q>(zz2, p.zz);
-  mul<P_q>(zz3, zz2, p.zz);
-  mul<P_q>(out, p.x, zz2);
-  mul<P_q>(out + 8, p.y, zz3);
-  cpy(out + 16, p.zzz);
+  uint32_t zz2[8], zz3[8], t[8];
+  qsqr(zz2, p.zz);
+  qmul(zz3, zz2, p.zz);
+  qmul(t, p.x, zz2);
+  from_rprime(out, t);
+  qmul(t, p.y, zz3);
+  from_rprime(out + 8, t);
+  from_rprime(out + 16, p.zzz);
 }
 
 __device__ __forceinline__ void ld_aff(aff_t& q, const fe* p) {

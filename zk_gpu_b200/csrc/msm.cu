@@ -285,6 +285,19 @@ __global__ void msm_combine_kernel(const fe* winsum, uint32_t windows, uint32_t 
   st_fe(out + 2, j + 16);
 }
 
+// bases (R form, as the API holds them) -> R' form for the curve arithmetic
+__global__ void msm_convert_bases_kernel(const fe* in, fe* out, uint64_t n) {
+  const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t x[8], y[8];
+  ld_fe(x, in + 2 * i);
+  ld_fe(y, in + 2 * i + 1);
+  to_rprime(x, x);
+  to_rprime(y, y);
+  st_fe(out + 2 * i, x);
+  st_fe(out + 2 * i + 1, y);
+}
+
 __global__ void zero_out_kernel(fe* out) {
   if (threadIdx.x < 3) {
     uint32_t z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -308,7 +321,7 @@ cudaError_t msm_run(const fe* d_scalars, const fe* d_bases, uint64_t n, fe* d_ou
   if (entries >= (1ull << 32)) return cudaErrorInvalidValue;  // entry offsets are 32-bit
   uint32_t *counts = nullptr, *offsets = nullptr, *cursor = nullptr, *bsums = nullptr, *list = nullptr;
   uint32_t *nsub = nullptr, *sub_off = nullptr, *sub2b = nullptr, *heavy = nullptr, *heavy_count = nullptr;
-  fe *buckets = nullptr, *segres = nullptr, *winsum = nullptr, *subres = nullptr;
+  fe *buckets = nullptr, *segres = nullptr, *winsum = nullptr, *subres = nullptr, *bases_rp = nullptr;
   const uint32_t segs = total / L;
   // sum_b ceil(count_b / SUB) <= entries / SUB + total; heavy buckets have > SEQ_MAX * SUB entries
   const uint64_t max_sub = entries / SUB + total + 1;
@@ -331,12 +344,14 @@ cudaError_t msm_run(const fe* d_scalars, const fe* d_bases, uint64_t n, fe* d_ou
   alloc((void**)&buckets, total * 128ull);
   alloc((void**)&segres, segs * 128ull);
   alloc((void**)&winsum, W * 128ull);
+  alloc((void**)&bases_rp, n * 64ull);
   if (e == cudaSuccess) {
     const double nd = (double)n;
     cudaMemsetAsync(counts, 0, total * 4ull, s);
     cudaMemsetAsync(heavy_count, 0, 4ull, s);
     const unsigned g = (unsigned)((n + 255) / 256);
     const unsigned gb = (total + 255) / 256;
+    msm_convert_bases_kernel<<<g, 256, 0, s>>>(d_bases, bases_rp, n);
     {
       ProfScope ps("msm_count", s, nd, nd * 32);
       msm_count_kernel<<<g, 256, 0, s>>>(d_scalars, n, (uint32_t)p.c, W, counts);
@@ -357,7 +372,7 @@ cudaError_t msm_run(const fe* d_scalars, const fe* d_bases, uint64_t n, fe* d_ou
       // convention: 6 Fq products per point-window (batch-affine cost)
       ProfScope ps("msm_bucket", s, (double)entries * 6, (double)entries * (64 + 4) + max_sub * 128.0);
       msm_subbucket_kernel<<<(unsigned)((max_sub + 255) / 256), 256, 0, s>>>(list, offsets, counts, sub_off, sub2b,
-                                                                              sub_off + total, d_bases, subres);
+                                                                              sub_off + total, bases_rp, subres);
     }
     {
       ProfScope ps("msm_bucket_final", s, (double)total * 14, total * 256.0);
@@ -370,12 +385,12 @@ cudaError_t msm_run(const fe* d_scalars, const fe* d_bases, uint64_t n, fe* d_ou
     }
     msm_window_kernel<<<W, 256, 0, s>>>(segres, winsum, B / L);
     msm_combine_kernel<<<1, 32, 0, s>>>(winsum, W, (uint32_t)p.c, d_out);
-    nl = 16;
+    nl = 17;
     e = cudaGetLastError();
   }
   for (void* ptr : {(void*)counts, (void*)offsets, (void*)cursor, (void*)bsums, (void*)list, (void*)nsub,
                     (void*)sub_off, (void*)sub2b, (void*)heavy, (void*)heavy_count, (void*)subres, (void*)buckets,
-                    (void*)segres, (void*)winsum})
+                    (void*)segres, (void*)winsum, (void*)bases_rp})
     if (ptr) cudaFreeAsync(ptr, s);
   if (launches) *launches = nl;
   return e;

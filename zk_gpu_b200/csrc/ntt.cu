@@ -711,9 +711,7 @@ int ntt_batch_grid(int device) {
 }
 
 cudaError_t ntt_batch_launch(const BatchPass* d_passes, uint32_t npass, uint32_t total_tiles, uint32_t* d_next,
-                             uint32_t* d_done, uint32_t* d_err, int grid, cudaStream_t s) {
-  // about two seconds at the B200 boost clock
-  const uint64_t spin_cycles = 4000000000ull;
+                             uint32_t* d_done, uint32_t* d_err, int grid, cudaStream_t s, uint64_t spin_cycles) {
   ntt_batch_kernel<<<grid, 256, batch_smem_bytes(), s>>>(d_passes, npass, total_tiles, d_next, d_done, d_err,
                                                          spin_cycles);
   return cudaGetLastError();

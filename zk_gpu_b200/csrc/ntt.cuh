@@ -101,8 +101,12 @@ struct BatchPass {
 };
 // Launch the persistent batch kernel over `npass` descriptors (device memory,
 // ordered by level), with counters next/done/err zeroed by the caller.
+// Every dependency wait gives up after spin_cycles SM clocks (default about
+// two seconds at the B200 boost clock), sets *d_err and stops the kernel.
+constexpr uint64_t NTT_BATCH_SPIN_CYCLES = 4000000000ull;
 cudaError_t ntt_batch_launch(const BatchPass* d_passes, uint32_t npass, uint32_t total_tiles, uint32_t* d_next,
-                             uint32_t* d_done, uint32_t* d_err, int grid, cudaStream_t s);
+                             uint32_t* d_done, uint32_t* d_err, int grid, cudaStream_t s,
+                             uint64_t spin_cycles = NTT_BATCH_SPIN_CYCLES);
 int ntt_batch_grid(int device);
 
 // Runs the NTT over d_a (2^log_n elements, in place).  d_tmp is scratch of
