@@ -163,20 +163,23 @@ __device__ __forceinline__ void ntt_pass_tile(const PassParams& p, uint64_t tile
     for (int k = 0; k < 9; k++) tws[k * (M / 2) + e] = wl[k];
   }
 
-  const uint64_t J = 1ull << p.log_J;
-  uint64_t o, col = 0, base, stride;
+  // element indices are < 2^28: 32-bit arithmetic, powers of two as shifts
+  const uint32_t t32 = (uint32_t)tile;
+  const uint32_t log_G = __ffs(G) - 1;
+  const uint32_t J = 1u << p.log_J;
+  uint32_t o, col = 0, base, stride;
   if (!p.is_final) {
-    const uint64_t cols_per_o = J / G;
-    o = tile / cols_per_o;
-    col = (tile % cols_per_o) * G + g;
-    base = o * (uint64_t)M * J + col;
+    const uint32_t log_cpo = p.log_J - log_G;  // columns per outer block = J / G
+    o = t32 >> log_cpo;
+    col = ((t32 & ((1u << log_cpo) - 1u)) << log_G) + g;
+    base = ((o << B) << p.log_J) + col;
     stride = J;
   } else {
-    const uint64_t rest_count = (1ull << p.log_O) >> p.log_m1;
-    const uint64_t rest = tile % rest_count;
-    const uint64_t k1 = (tile / rest_count) * G + g;
-    o = k1 * rest_count + rest;
-    base = o * M;
+    const uint32_t log_rest = p.log_O - p.log_m1;  // rest_count = O / m_1
+    const uint32_t rest = t32 & ((1u << log_rest) - 1u);
+    const uint32_t k1 = ((t32 >> log_rest) << log_G) + g;
+    o = (k1 << log_rest) + rest;
+    base = o << B;
     stride = 1;
   }
 
@@ -185,9 +188,9 @@ __device__ __forceinline__ void ntt_pass_tile(const PassParams& p, uint64_t tile
 #pragma unroll
     for (int r = 0; r < 8; r++) {
       if (BATCH)
-        ld_fe_cg(x[r], p.in + base + (uint64_t)(q + T * r) * stride);
+        ld_fe_cg(x[r], p.in + (base + (q + T * r) * stride));
       else
-        ld_fe(x[r], p.in + base + (uint64_t)(q + T * r) * stride);
+        ld_fe(x[r], p.in + (base + (q + T * r) * stride));
     }
   } else {
 #pragma unroll
@@ -195,10 +198,10 @@ __device__ __forceinline__ void ntt_pass_tile(const PassParams& p, uint64_t tile
   }
 
   if (p.pre_lo && active) {
-    const uint64_t mask = (1ull << p.pre_shift) - 1;
+    const uint32_t mask = (1u << p.pre_shift) - 1u;
 #pragma unroll
     for (int r = 0; r < 8; r++) {
-      const uint64_t xi = base + (uint64_t)(q + T * r) * stride;  // first pass: global input index
+      const uint32_t xi = base + (q + T * r) * stride;  // first pass: global input index
       uint32_t a[8], b[8];
       ld_fe_nc(a, p.pre_lo + (xi & mask));
       ld_fe_nc(b, p.pre_hi + (xi >> p.pre_shift));
@@ -217,13 +220,14 @@ __device__ __forceinline__ void ntt_pass_tile(const PassParams& p, uint64_t tile
     for (int r = 0; r < 8; r++) {
       const uint32_t k = __brev(8 * q + r) >> (32 - B);
       uint32_t w[8];
-      ld_fe_nc(w, p.twist + (uint64_t)k * J + col);
+      const uint32_t kj = (k << p.log_J) + col;
+      ld_fe_nc(w, p.twist + kj);
       mul_r29<P_r>(x[r], x[r], w);
-      st_fe(p.out + o * (uint64_t)M * J + (uint64_t)k * J + col, x[r]);
+      st_fe(p.out + (((o << B) << p.log_J) + kj), x[r]);
     }
   } else {
     // rev(o): o = k_1 * 2^(b_2+..) + ... + k_(p-1);  rev = k_1 + 2^b_1 k_2 + ...
-    uint64_t rev = 0, rem = o;
+    uint32_t rev = 0, rem = o;
     uint32_t low_bits = 0, total = 0;
 #pragma unroll
     for (int t = 0; t < NTT_MAX_PASS; t++)
@@ -233,8 +237,8 @@ __device__ __forceinline__ void ntt_pass_tile(const PassParams& p, uint64_t tile
     for (int t = 0; t < NTT_MAX_PASS; t++) {
       if (t < (int)p.nprev) {
         above -= p.prev_bits[t];
-        const uint64_t digit = rem >> above;
-        rem &= (1ull << above) - 1;
+        const uint32_t digit = rem >> above;
+        rem &= (1u << above) - 1u;
         rev |= digit << low_bits;
         low_bits += p.prev_bits[t];
       }
@@ -249,7 +253,7 @@ __device__ __forceinline__ void ntt_pass_tile(const PassParams& p, uint64_t tile
       } else {
         reduce_once<P_r>(v, x[r]);
       }
-      st_fe(p.out + rev + ((uint64_t)k << total), v);
+      st_fe(p.out + (rev + (k << total)), v);
     }
   }
 }
