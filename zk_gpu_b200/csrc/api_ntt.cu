@@ -77,12 +77,43 @@ int ntt_host(int device, uint64_t* a, uint32_t log_n, const uint64_t* omega, con
 int lde_device(int device, const fe* d_values, uint32_t log_n, fe* d_ext, uint32_t log_ext, const hf::Fr& w_inv,
                const hf::Fr& divisor, const hf::Fr& g, const hf::Fr& w_ext, cudaStream_t s) {
   const size_t n = (size_t)1 << log_n, N = (size_t)1 << log_ext;
-  // coefficients in the first n slots of d_ext, zero tail
-  ZK_TRY("lde copy", cudaMemcpyAsync(d_ext, d_values, n * sizeof(fe), cudaMemcpyDeviceToDevice, s));
-  if (N > n) ZK_TRY("lde zero", cudaMemsetAsync(d_ext + n, 0, (N - n) * sizeof(fe), s));
-  int st = ntt_device(device, d_ext, log_n, w_inv, nullptr, &divisor, s);
-  if (st) return st;
-  return ntt_device(device, d_ext, log_ext, w_ext, &g, nullptr, s);
+  if (log_n < 3) {
+    // tiny domains: coefficients in the first n slots, zero tail, two transforms
+    ZK_TRY("lde copy", cudaMemcpyAsync(d_ext, d_values, n * sizeof(fe), cudaMemcpyDeviceToDevice, s));
+    if (N > n) ZK_TRY("lde zero", cudaMemsetAsync(d_ext + n, 0, (N - n) * sizeof(fe), s));
+    int st = ntt_device(device, d_ext, log_n, w_inv, nullptr, &divisor, s);
+    if (st) return st;
+    return ntt_device(device, d_ext, log_ext, w_ext, &g, nullptr, s);
+  }
+  // 1) ifft of the values, read in place from d_values, written to d_ext[0, n);
+  //    its last pass multiplies output i by n^-1 * g^i (the coset shift)
+  // 2) NTT of d_ext on the extended domain; its first pass treats the zero
+  //    padding [n, N) as known zeros, so the tail is never written or read
+  cudaError_t e;
+  const zk::NttTables* ti = zk::ntt_tables_get(device, w_inv, (int)log_n, s, &e);
+  if (!ti) return zk::status_of("ntt_tables_get", e);
+  const zk::NttTables* te = zk::ntt_tables_get(device, w_ext, (int)log_ext, s, &e);
+  if (!te) return zk::status_of("ntt_tables_get", e);
+  const zk::PowTables* gd = zk::pow_tables_get(device, g, (int)log_n, s, &e, &divisor);
+  if (!gd) return zk::status_of("pow_tables_get", e);
+  fe* tmp = nullptr;
+  ZK_TRY("cudaMallocAsync(lde scratch)", cudaMallocAsync((void**)&tmp, N * sizeof(fe), s));
+  // the skip works on whole rows of the first pass; otherwise zero the tail
+  if (te->plan.npass > 1 && N > n && n % (1ull << (log_ext - te->plan.bits[0])) != 0)
+    ZK_TRY("lde zero", cudaMemsetAsync(d_ext + n, 0, (N - n) * sizeof(fe), s));
+  zk::NttFuse f1;
+  f1.src = d_values;
+  f1.post_tab = gd;
+  e = zk::ntt_run(*ti, d_ext, tmp, f1, s);
+  zk::count_launches(ti->plan.npass);
+  if (e == cudaSuccess) {
+    zk::NttFuse f2;
+    f2.nonzero = n;
+    e = zk::ntt_run(*te, d_ext, tmp, f2, s);
+    zk::count_launches(te->plan.npass);
+  }
+  cudaFreeAsync(tmp, s);
+  return zk::status_of("lde", e);
 }
 
 }  // namespace

@@ -24,9 +24,10 @@ namespace zk {
 namespace {
 struct PowKey {
   int dev, log_n;
-  uint64_t c[4];
+  uint64_t c[4], s[4];
   bool operator<(const PowKey& o) const {
-    return std::tie(dev, log_n, c[0], c[1], c[2], c[3]) < std::tie(o.dev, o.log_n, o.c[0], o.c[1], o.c[2], o.c[3]);
+    return std::tie(dev, log_n, c[0], c[1], c[2], c[3], s[0], s[1], s[2], s[3]) <
+           std::tie(o.dev, o.log_n, o.c[0], o.c[1], o.c[2], o.c[3], o.s[0], o.s[1], o.s[2], o.s[3]);
   }
 };
 std::mutex g_pow_mu;
@@ -35,8 +36,11 @@ std::map<PowKey, PowTables> g_pow_cache;
 
 // Coset power tables cached per (device, c, log_n): batches and the serving
 // loop reuse the same few cosets (the field generator and its shifts).
-const PowTables* pow_tables_get(int device, const host::Fr& c, int log_n, cudaStream_t s, cudaError_t* err) {
-  PowKey k{device, log_n, {c.v[0], c.v[1], c.v[2], c.v[3]}};
+const PowTables* pow_tables_get(int device, const host::Fr& c, int log_n, cudaStream_t s, cudaError_t* err,
+                                const host::Fr* scale) {
+  const host::Fr one = host::one();
+  const host::Fr& sc = scale ? *scale : one;
+  PowKey k{device, log_n, {c.v[0], c.v[1], c.v[2], c.v[3]}, {sc.v[0], sc.v[1], sc.v[2], sc.v[3]}};
   std::lock_guard<std::mutex> lk(g_pow_mu);
   auto it = g_pow_cache.find(k);
   if (it != g_pow_cache.end()) {
@@ -44,7 +48,7 @@ const PowTables* pow_tables_get(int device, const host::Fr& c, int log_n, cudaSt
     return &it->second;
   }
   PowTables t;
-  cudaError_t e = pow_tables_make(&t, c, log_n, s);
+  cudaError_t e = pow_tables_make(&t, c, log_n, s, scale);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   *err = e;
   if (e != cudaSuccess) return nullptr;

@@ -185,9 +185,12 @@ __device__ __forceinline__ void ntt_pass_tile(const PassParams& p, uint64_t tile
 
   uint32_t x[8][8];
   if (active) {
+    const uint32_t rows = p.in_rows ? p.in_rows : M;  // rows past in_rows are zero padding
 #pragma unroll
     for (int r = 0; r < 8; r++) {
-      if (BATCH)
+      if (q + T * r >= rows)
+        set_zero(x[r]);
+      else if (BATCH)
         ld_fe_cg(x[r], p.in + (base + (q + T * r) * stride));
       else
         ld_fe(x[r], p.in + (base + (q + T * r) * stride));
@@ -247,13 +250,21 @@ __device__ __forceinline__ void ntt_pass_tile(const PassParams& p, uint64_t tile
     for (int r = 0; r < 8; r++) {
       const uint32_t k = __brev(8 * q + r) >> (32 - B);
       uint32_t v[8];
-      if (p.has_post) {
+      const uint32_t kout = rev + (k << total);  // natural output index
+      if (p.post_lo) {
+        uint32_t a[8], b[8];
+        ld_fe_nc(a, p.post_lo + (kout & ((1u << p.post_shift) - 1u)));
+        ld_fe_nc(b, p.post_hi + (kout >> p.post_shift));
+        mul_r29<P_r>(a, a, b);
+        mul_r29<P_r>(v, x[r], a);
+        reduce_once<P_r>(v, v);
+      } else if (p.has_post) {
         mul_r29<P_r>(v, x[r], p.post.w);
         reduce_once<P_r>(v, v);
       } else {
         reduce_once<P_r>(v, x[r]);
       }
-      st_fe(p.out + (rev + (k << total)), v);
+      st_fe(p.out + kout, v);
     }
   }
 }
@@ -450,8 +461,25 @@ static cudaError_t pow_two_level(fe** lo, fe** hi, uint32_t* shift, const host::
   return cudaGetLastError();
 }
 
-cudaError_t pow_tables_make(PowTables* t, const host::Fr& c, int log_n, cudaStream_t s) {
-  return pow_two_level(&t->lo, &t->hi, &t->shift, c, log_n, s, true);
+// t[i] *= scale (R' form)
+__global__ void scale_table_kernel(fe* t, fe scale, uint64_t count) {
+  const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  uint32_t v[8];
+  ld_fe(v, t + i);
+  mul_r29<P_r>(v, v, scale.w);
+  reduce_once<P_r>(v, v);
+  st_fe(t + i, v);
+}
+
+cudaError_t pow_tables_make(PowTables* t, const host::Fr& c, int log_n, cudaStream_t s, const host::Fr* scale) {
+  cudaError_t e = pow_two_level(&t->lo, &t->hi, &t->shift, c, log_n, s, true);
+  if (e == cudaSuccess && scale) {
+    const uint64_t nlo = 1ull << t->shift;
+    scale_table_kernel<<<(unsigned)((nlo + 255) / 256), 256, 0, s>>>(t->lo, to_fe_rp(*scale), nlo);
+    e = cudaGetLastError();
+  }
+  return e;
 }
 void pow_tables_free(PowTables* t, cudaStream_t s) {
   if (t->lo) cudaFreeAsync(t->lo, s);
@@ -621,6 +649,15 @@ static cudaError_t dispatch_pass(int B, const PassParams& pp, uint64_t ncta, cud
 
 uint64_t ntt_pass_params(const NttTables& t, int k, fe* d_a, fe* d_tmp, const PowTables* pre, const host::Fr* post,
                          PassParams* out) {
+  NttFuse f;
+  f.pre = pre;
+  f.post = post;
+  return ntt_pass_params(t, k, d_a, d_tmp, f, out);
+}
+
+uint64_t ntt_pass_params(const NttTables& t, int k, fe* d_a, fe* d_tmp, const NttFuse& f, PassParams* out) {
+  const PowTables* pre = f.pre;
+  const host::Fr* post = f.post;
   const NttPlan& p = t.plan;
   const int L = p.log_n;
   int done = 0;
@@ -647,6 +684,16 @@ uint64_t ntt_pass_params(const NttTables& t, int k, fe* d_a, fe* d_tmp, const Po
     pp.has_post = 1;
     pp.post = to_fe_rp(*post);
   }
+  if (final_pass && f.post_tab) {
+    pp.post_lo = f.post_tab->lo;
+    pp.post_hi = f.post_tab->hi;
+    pp.post_shift = f.post_tab->shift;
+  }
+  if (k == 0 && f.nonzero) {
+    // first pass reads rows of J = 2^(L - b) elements: whole zero rows are skipped
+    const uint64_t J = 1ull << (L - b);
+    if (f.nonzero % J == 0 && f.nonzero / J < (1ull << b)) pp.in_rows = (uint32_t)(f.nonzero / J);
+  }
   // buffers: single pass in place; otherwise a -> tmp, tmp in place, tmp -> a
   if (p.npass == 1) {
     pp.in = d_a;
@@ -661,6 +708,7 @@ uint64_t ntt_pass_params(const NttTables& t, int k, fe* d_a, fe* d_tmp, const Po
     pp.in = d_tmp;
     pp.out = d_a;
   }
+  if (k == 0 && f.src) pp.in = f.src;  // out of place: the first pass reads the source
   const uint32_t Gmax = b >= 11 ? 1u : (1u << (11 - b));
   uint64_t groups_dim;
   if (!final_pass) {
@@ -676,9 +724,19 @@ uint64_t ntt_pass_params(const NttTables& t, int k, fe* d_a, fe* d_tmp, const Po
 }
 
 cudaError_t ntt_run(const NttTables& t, fe* d_a, fe* d_tmp, const PowTables* pre, const host::Fr* post, cudaStream_t s) {
+  NttFuse f;
+  f.pre = pre;
+  f.post = post;
+  return ntt_run(t, d_a, d_tmp, f, s);
+}
+
+cudaError_t ntt_run(const NttTables& t, fe* d_a, fe* d_tmp, const NttFuse& f, cudaStream_t s) {
+  const PowTables* pre = f.pre;
+  const host::Fr* post = f.post;
   const NttPlan& p = t.plan;
   const int L = p.log_n;
   if (L <= 2) {
+    if (f.post_tab) return cudaErrorInvalidValue;  // the direct kernel takes constant scales only
     fe po{};
     if (post) po = to_fe_rp(*post);
     ntt_tiny_kernel<<<1, 32, 0, s>>>(d_a, (uint32_t)L, to_fe(t.omega), pre ? pre->lo : nullptr, pre ? pre->hi : nullptr,
@@ -690,7 +748,7 @@ cudaError_t ntt_run(const NttTables& t, fe* d_a, fe* d_tmp, const PowTables* pre
   for (int k = 0; k < p.npass; k++) {
     const int b = p.bits[k];
     PassParams pp;
-    const uint64_t ncta = ntt_pass_params(t, k, d_a, d_tmp, pre, post, &pp);
+    const uint64_t ncta = ntt_pass_params(t, k, d_a, d_tmp, f, &pp);
     const double nel = (double)(1ull << L);
     // algorithmic work: radix-2 convention (n/2) * b products; bytes: read + write (+ twist table)
     ProfScope prof(names[b], s, nel / 2 * b, nel * 32.0 * (pp.is_final ? 2 : 3));

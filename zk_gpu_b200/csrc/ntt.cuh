@@ -59,12 +59,15 @@ const NttTables* ntt_tables_get(int device, const host::Fr& omega, int log_n, cu
 // `cap` elements (no allocation); ntt_tables_elems gives the size needed.
 size_t ntt_tables_elems(int log_n);
 cudaError_t ntt_tables_fill(NttTables* t, const host::Fr& omega, int log_n, fe* mem, size_t cap, cudaStream_t s);
-// Two-level power tables for c^x, x < 2^log_n, allocated from the stream pool
-// (caller frees with pow_tables_free on the same stream).
-cudaError_t pow_tables_make(PowTables* t, const host::Fr& c, int log_n, cudaStream_t s);
+// Two-level power tables for scale * c^x, x < 2^log_n (scale folded into the
+// low table; null = 1), allocated from the stream pool (caller frees with
+// pow_tables_free on the same stream).
+cudaError_t pow_tables_make(PowTables* t, const host::Fr& c, int log_n, cudaStream_t s,
+                            const host::Fr* scale = nullptr);
 void pow_tables_free(PowTables* t, cudaStream_t s);
-// Cached (device, c, log_n) power tables, owned by the cache.
-const PowTables* pow_tables_get(int device, const host::Fr& c, int log_n, cudaStream_t s, cudaError_t* err);
+// Cached (device, c, log_n, scale) power tables, owned by the cache.
+const PowTables* pow_tables_get(int device, const host::Fr& c, int log_n, cudaStream_t s, cudaError_t* err,
+                                const host::Fr* scale = nullptr);
 
 // Parameters of one pass launch (kernel argument / batch descriptor).
 struct PassParams {
@@ -84,11 +87,27 @@ struct PassParams {
   uint32_t is_final;
   uint32_t has_post;
   fe post;  // R' form
+  // final pass: output k multiplied by post_lo[k & mask] * post_hi[k >> shift]
+  const fe* post_lo;
+  const fe* post_hi;
+  uint32_t post_shift;
+  // first pass: rows >= in_rows are known zeros (zero-padded input), 0 = all
+  uint32_t in_rows;
+};
+
+// Optional work fused into a transform.
+struct NttFuse {
+  const PowTables* pre = nullptr;       // input i times c^i
+  const host::Fr* post = nullptr;       // every output times a constant
+  const PowTables* post_tab = nullptr;  // output k times the table's k-th power
+  uint64_t nonzero = 0;                 // only inputs [0, nonzero) may be non-zero (0 = all)
+  const fe* src = nullptr;              // read the input from here instead of d_a (d_a gets the result)
 };
 
 // Pass k of the plan in `t` over d_a / d_tmp; returns its CTA count.
 uint64_t ntt_pass_params(const NttTables& t, int k, fe* d_a, fe* d_tmp, const PowTables* pre, const host::Fr* post,
                          PassParams* pp);
+uint64_t ntt_pass_params(const NttTables& t, int k, fe* d_a, fe* d_tmp, const NttFuse& f, PassParams* pp);
 
 // One pass of one transform inside a batch launch.
 struct BatchPass {
@@ -115,6 +134,7 @@ int ntt_batch_grid(int device);
 // output; outputs are canonical.
 cudaError_t ntt_run(const NttTables& t, fe* d_a, fe* d_tmp, const PowTables* pre, const host::Fr* post,
                     cudaStream_t s);
+cudaError_t ntt_run(const NttTables& t, fe* d_a, fe* d_tmp, const NttFuse& f, cudaStream_t s);
 
 // Number of launches ntt_run issues for a plan (for launch accounting).
 inline int ntt_launches(const NttPlan& p) { return p.npass; }

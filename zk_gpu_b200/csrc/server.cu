@@ -239,6 +239,8 @@ class Server {
       const PowTables* pre;
       host::Fr post;
       bool has_post;
+      const PowTables* post_tab;  // final pass: output i times table power i
+      uint64_t nonzero;           // first pass: inputs past this are zero padding
       int level0;
       int dep_job;  // index in items of the transform this one follows, or -1
     };
@@ -272,7 +274,6 @@ class Server {
       frees_ntt.push_back(d);
       frees_ntt.push_back(tmp);
       ok(cudaMemcpyAsync(d, j.input, n * 32, cudaMemcpyHostToDevice, w.s_ntt));
-      if (N > n) ok(cudaMemsetAsync(d + n, 0, (N - n) * 32, w.s_ntt));
       cudaError_t te;
       if (!lde) {
         NttItem it{};
@@ -294,23 +295,28 @@ class Server {
         it.dep_job = -1;
         items.push_back(it);
       } else {
+        // ifft in place on the first n slots; its last pass applies n^-1 g^i,
+        // and the extended NTT skips the zero padding (as zkgpu_lagrange_to_extended)
         NttItem a{}, b{};
+        const host::Fr div = fr_of(j.scale);
         a.t = ntt_tables_get(device_, fr_of(j.omega), (int)j.log_n, w.s_ntt, &te);
         b.t = ntt_tables_get(device_, fr_of(j.omega_ext), (int)j.log_ext, w.s_ntt, &te);
-        b.pre = pow_tables_get(device_, fr_of(j.coset), (int)j.log_ext, w.s_ntt, &te);
-        if (!a.t || !b.t || !b.pre) {
+        a.post_tab = pow_tables_get(device_, fr_of(j.coset), (int)j.log_n, w.s_ntt, &te, &div);
+        if (!a.t || !b.t || !a.post_tab) {
           ok(te == cudaSuccess ? cudaErrorInvalidValue : te);
           break;
         }
-        a.data = d;  // ifft in place on the first n slots of the extended buffer
+        if (b.t->plan.npass > 1 && N > n && n % (1ull << (j.log_ext - b.t->plan.bits[0])) != 0)
+          ok(cudaMemsetAsync(d + n, 0, (N - n) * 32, w.s_ntt));
+        a.data = d;
         a.tmp = tmp;
-        a.has_post = true;
-        a.post = fr_of(j.scale);
+        a.has_post = false;
         a.level0 = 0;
         a.dep_job = -1;
         b.data = d;
         b.tmp = tmp;
         b.has_post = false;
+        b.nonzero = n;
         b.level0 = a.t->plan.npass;
         b.dep_job = (int)items.size();
         items.push_back(a);
@@ -330,8 +336,12 @@ class Server {
           const int k = lvl - it.level0;
           if (k < 0 || k >= it.t->plan.npass) continue;
           BatchPass bp{};
-          const uint64_t ncta =
-              ntt_pass_params(*it.t, k, it.data, it.tmp, it.pre, it.has_post ? &it.post : nullptr, &bp.p);
+          NttFuse fu;
+          fu.pre = it.pre;
+          fu.post = it.has_post ? &it.post : nullptr;
+          fu.post_tab = it.post_tab;
+          fu.nonzero = it.nonzero;
+          const uint64_t ncta = ntt_pass_params(*it.t, k, it.data, it.tmp, fu, &bp.p);
           bp.B = (uint32_t)it.t->plan.bits[k];
           bp.ntiles = (uint32_t)ncta;
           bp.tile_base = (uint32_t)tiles;
