@@ -245,6 +245,18 @@ def run_ours(args, rank: int, world: int, local_rank: int):
 
     imad_ps, modmul_ps = zk.int_peak(dev)
 
+    # autotuner (untimed): NTT plans for the LDE's two sizes, the MSM window
+    # for 2^22, and batched-transform plans for 2^10..2^20
+    tune = {"ms": 0.0}
+    if not args.no_tune:
+        tune["ms"] += zk.autotune(zk.TUNE_NTT, LOG_N, LOG_N, device=dev)
+        tune["ms"] += zk.autotune(zk.TUNE_NTT, LOG_EXT, LOG_EXT, device=dev)
+        tune["ms"] += zk.autotune(zk.TUNE_MSM, 22, 22, device=dev)
+        tune["ms"] += zk.autotune(zk.TUNE_NTT_BATCHED, 10, 20, device=dev)
+    tune["ntt_plans"] = {str(k): zk.get_ntt_plan(k, device=dev) for k in list(range(10, 21)) + [LOG_N, LOG_EXT]}
+    tune["msm_window_2p22"] = zk.get_msm_window(22, device=dev)
+    tune["ms"] = round(tune["ms"], 1)
+
     def step():
         zk.lagrange_to_extended_dev(d_vals, d_ext, LOG_N, LOG_EXT, c["omega_inv"], c["divisor"], c["g"],
                                     c["omega_ext"], stream=stream)
@@ -297,7 +309,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     sc = rand_fr(n_msm, 4242 + rank)
     sc[: n_msm // 10] = small_fr(n_msm // 10, 4343 + rank)
     d_sc = torch.from_numpy(sc.view(np.int64)).to(f"cuda:{dev}")
-    d_bs = torch.from_numpy(gen_bases_tiled(n_msm).view(np.int64)).to(f"cuda:{dev}")
+    d_bs = gen_bases(zk, torch, n_msm, 4141 + rank, dev)
     d_out = torch.zeros(12, dtype=torch.int64, device=f"cuda:{dev}")
     zk.msm_dev(d_sc, d_bs, d_out, stream=stream)
     stream.synchronize()
@@ -369,9 +381,12 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                   "ntt_fwd_2p24_ms": round(ntt_ms, 4),
                   "msm_2p22_mpts_s": round(world * n_msm / (msm_ms * 1e-3) / 1e6, 2),
                   "msm_2p22_ms": round(msm_ms, 3),
+                  "msm_inputs": "bases k_i*(1,2) for seeded uniform Fr k_i (device fixed-base multiplication); "
+                                "scalars uniform Fr, 10% replaced by uniform < 2^16",
                   "msm_kernels": {k: {"launches": v["launches"], "ms": round(v["ms"], 3)} for k, v in msm_prof.items()},
                   "msm_roofline": msm_roofline(msm_prof, imad_ps, n_msm, msm_ms),
                   "batched_ntt": batched,
+                  "autotune": tune,
                   "serving": serving},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -507,7 +522,7 @@ def bench_serving(zk, torch, dev: int, njobs: int = 1000, rate: float = 2000.0, 
             to, o = pinned(1 << (k + 2 if kind == "lde" else k), 4)
         pools[key] = (ti, a, to, o)
     nb = 1 << 20
-    bases = gen_bases_tiled(nb)
+    bases = gen_bases(zk, torch, nb, 4545, dev).cpu().numpy().view(np.uint64)
 
     def make_job(kind, k):
         ti, a, to, o = pools[(kind, k)]
@@ -682,7 +697,7 @@ def run_case(args):
     elif args.case == "msm20":
         n = 1 << 20
         s = torch.from_numpy(rand_fr(n, 8).view(np.int64)).cuda()
-        b = torch.from_numpy(gen_bases_tiled(n).view(np.int64)).cuda()
+        b = gen_bases(zk, torch, n, 4141, 0)
         out = torch.zeros(12, dtype=torch.int64, device="cuda")
 
         def step():
@@ -699,28 +714,14 @@ def run_case(args):
     return 0
 
 
-def gen_bases_tiled(n: int, distinct: int = 4096) -> np.ndarray:
-    """n affine points: the multiples (i + 1) * G for i < `distinct`, built by
-    repeated addition on the host with Python ints, tiled to length n."""
-    q = 21888242871839275222246405745257275088696311157297823662689037894645226208583
-    d = min(n, distinct)
-    out = np.empty((d, 8), np.uint64)
-    x, y = 1, 2
-    gx, gy = 1, 2
-    rq = (1 << 256) % q
-    m = 2**64 - 1
-    for i in range(d):
-        xm, ym = x * rq % q, y * rq % q
-        out[i] = [(xm >> (64 * j)) & m for j in range(4)] + [(ym >> (64 * j)) & m for j in range(4)]
-        if x == gx:
-            lam = 3 * x * x * pow(2 * y, -1, q) % q
-        else:
-            lam = (gy - y) * pow(gx - x, -1, q) % q
-        x3 = (lam * lam - x - gx) % q
-        y = (lam * (x - x3) - y) % q
-        x = x3
-    reps = (n + d - 1) // d
-    return np.ascontiguousarray(np.tile(out, (reps, 1))[:n])
+def gen_bases(zk, torch, n: int, seed: int, dev: int):
+    """n affine G1 bases k_i * (1, 2) for seeded uniform Fr k_i, generated on
+    the device by the library's fixed-base multiplication (device tensor)."""
+    k = torch.from_numpy(rand_fr(n, seed).view(np.int64)).to(f"cuda:{dev}")
+    out = torch.empty((n, 8), dtype=torch.int64, device=f"cuda:{dev}")
+    zk.g1_mul_fixed_dev(k, out)
+    del k
+    return out
 
 
 def main():
@@ -731,6 +732,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-loop sub-benchmark")
+    ap.add_argument("--no-tune", action="store_true", help="use the built-in NTT plans and MSM windows")
     ap.add_argument("--case", choices=["ntt22", "ntt24", "lde20", "msm20"], default=None,
                     help="run a small profiling case instead of the benchmark")
     args = ap.parse_args()

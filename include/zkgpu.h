@@ -101,6 +101,13 @@ int zkgpu_msm(int device, const uint64_t *scalars, const uint64_t *bases_xy, uin
 int zkgpu_lagrange_to_extended(int device, const uint64_t *values, uint32_t log_n, uint64_t *ext, uint32_t log_ext,
                                const uint64_t omega_inv[4], const uint64_t divisor[4], const uint64_t g[4],
                                const uint64_t omega_ext[4]);
+/* The inverse step, halo2 extended -> coefficients (the quotient polynomial's
+ * path back from the extended domain):
+ *   a = ifft(ext, omega_ext_inv, ext_divisor = 2^-log_ext);  a[i] *= g_inv^i;
+ *   out = a[0, m)                                             (truncate, m <= 2^log_ext)
+ * ext: 2^log_ext host elements (read only); out: m host elements. */
+int zkgpu_extended_to_coeff(int device, const uint64_t *ext, uint32_t log_ext, uint64_t *out, uint64_t m,
+                            const uint64_t omega_ext_inv[4], const uint64_t ext_divisor[4], const uint64_t g_inv[4]);
 
 /* ======================================================================
  * Device-resident API: pointers are device memory on `device`, work is
@@ -115,6 +122,9 @@ int zkgpu_ntt_dev(int device, uint64_t *d_a, uint32_t log_n, const uint64_t omeg
 int zkgpu_lagrange_to_extended_dev(int device, const uint64_t *d_values, uint32_t log_n, uint64_t *d_ext,
                                    uint32_t log_ext, const uint64_t omega_inv[4], const uint64_t divisor[4],
                                    const uint64_t g[4], const uint64_t omega_ext[4], void *stream);
+int zkgpu_extended_to_coeff_dev(int device, const uint64_t *d_ext, uint32_t log_ext, uint64_t *d_out, uint64_t m,
+                                const uint64_t omega_ext_inv[4], const uint64_t ext_divisor[4], const uint64_t g_inv[4],
+                                void *stream);
 /* No counterpart in the reference.  The same in-place NTT as zkgpu_ntt_dev
  * (no coset, no scale) for callers that cannot allocate device memory — code
  * running under stream capture, or inside a runtime that owns every device
@@ -130,6 +140,12 @@ int zkgpu_ntt_dev_static(int device, uint64_t *d_a, uint32_t log_n, const uint64
 /* d_out_xyz receives the Jacobian sum (12 words, device memory) */
 int zkgpu_msm_dev(int device, const uint64_t *d_scalars, const uint64_t *d_bases_xy, uint64_t n, uint64_t *d_out_xyz,
                   void *stream);
+/* d_out_xy[i] = k_i * base (affine, Fq Montgomery, (0, 0) for the identity),
+ * k_i = d_scalars[i] (Fr Montgomery); base_xy is a host value.  Generates MSM
+ * bases as multiples of a fixed point, e.g. of the generator (1, 2).
+ * Synchronous on `stream`. */
+int zkgpu_g1_mul_fixed_dev(int device, const uint64_t base_xy[8], const uint64_t *d_scalars, uint64_t n,
+                           uint64_t *d_out_xy, void *stream);
 
 /* ======================================================================
  * Batched NTTs: many transforms of uneven sizes in one persistent launch,
@@ -155,6 +171,34 @@ int zkgpu_ntt_batch_run(void *handle, void *stream);
 int zkgpu_ntt_batch_check(void *handle);
 void zkgpu_ntt_batch_info(void *handle, uint32_t *passes, uint32_t *tiles, int *grid);
 void zkgpu_ntt_batch_destroy(void *handle);
+
+/* ======================================================================
+ * Autotuner: per device and size, the NTT plan (pass widths b_k, 3..11 bits;
+ * each pass runs radix-2^b_k columns in CTA tiles of 2^b_k x G elements,
+ * G = 2^(11 - b_k)) and the MSM window width c, picked by timing candidates
+ * on the device.  Replaces the fixed 1024 x n/1024 split of
+ * cuda/fft.cu:275-405 and the ceil(ln len) window of cuda/fft.cu:165-172.
+ * Choices change speed only: every plan and window is bit-exact.  Installed
+ * choices apply to later calls on that device (tables of a new plan are built
+ * on first use).
+ * ====================================================================== */
+#define ZKGPU_TUNE_NTT 1u         /* time one transform per size */
+#define ZKGPU_TUNE_MSM 2u         /* time MSMs of 2^log_n points */
+#define ZKGPU_TUNE_NTT_BATCHED 4u /* time batches of transforms of each size (the batcher's case) */
+/* Tune sizes 2^log_min .. 2^log_max; reps timed runs per candidate (0 = 3);
+ * *ms_spent (nullable) receives the device time the tuning took. */
+int zkgpu_autotune(int device, uint32_t what, uint32_t log_min, uint32_t log_max, uint32_t reps, double *ms_spent);
+/* Install a plan (npass = 0: back to the built-in plan for log_n > 2) /
+ * read the plan used for (device, log_n).  EINVAL for unsupported plans. */
+int zkgpu_tune_set_ntt_plan(int device, uint32_t log_n, uint32_t npass, const uint32_t bits[4]);
+int zkgpu_tune_get_ntt_plan(int device, uint32_t log_n, uint32_t *npass, uint32_t bits[4]);
+/* Install (c = 0: clear) / read the MSM window for 2^log_n points. */
+int zkgpu_tune_set_msm_window(int device, uint32_t log_n, uint32_t c);
+int zkgpu_tune_get_msm_window(int device, uint32_t log_n, uint32_t *c);
+/* Persist the device's installed choices; load installs the entries recorded
+ * for a device of the same name and SM count (*loaded = entries installed). */
+int zkgpu_tune_save(int device, const char *path);
+int zkgpu_tune_load(int device, const char *path, uint32_t *loaded);
 
 /* ======================================================================
  * Serving loop: continuous batching with HBM-budget admission.  Replaces the

@@ -210,6 +210,16 @@ def coeff_to_extended(a: np.ndarray, log_n: int, log_ext: int, g, w_ext, threads
     return ext
 
 
+def extended_to_coeff(ext: np.ndarray, log_ext: int, m: int, w_ext_inv, ext_divisor, g_inv,
+                      threads: int = 0) -> np.ndarray:
+    """halo2 EvaluationDomain::extended_to_coeff (halo2_proofs/src/poly/domain.rs,
+    the external halo2 fork the reference's callers use): ifft over the
+    extended domain, distribute powers of g^-1 (undo the coset), truncate to m."""
+    a = ifft(ext, w_ext_inv, log_ext, ext_divisor, threads)
+    a = distribute_powers(a, g_inv, threads)
+    return np.ascontiguousarray(a[:m])
+
+
 def twiddle_lut(w, log_n: int, sparse_degree: int = 10, with_last_level: bool = True) -> np.ndarray:
     w = _e(w)
     n = lib().zko_twiddle_lut(None, _p(w), log_n, sparse_degree, int(with_last_level))

@@ -109,3 +109,26 @@ def test_msm_device_api(zk, oracle):
     torch.cuda.synchronize()
     jac = out.cpu().numpy().view(np.uint64)
     assert np.array_equal(oracle.g1_normalize(jac), oracle.multiexp(s, pts))
+
+
+def test_g1_mul_fixed_matches_oracle_bases(zk, oracle):
+    """k_i * (1, 2) on the device (the MSM-bases generator) equals the
+    oracle's fixed-base multiples for the same seeded k_i, bit-exact, with
+    the edge scalars 0 (identity (0, 0)), 1 (the generator) and r - 1 (-G)."""
+    import torch
+    n = 5000
+    pts, k = oracle.rand_bases(n, 31, with_dlog=True)
+    r = B.R_MOD
+    k[0] = oracle.to_mont(0)
+    k[1] = oracle.to_mont(1)
+    k[2] = oracle.to_mont(r - 1)
+    d_k = torch.from_numpy(k.view(np.int64)).cuda()
+    d_out = torch.empty((n, 8), dtype=torch.int64, device="cuda")
+    zk.g1_mul_fixed_dev(d_k, d_out)
+    got = d_out.cpu().numpy().view(np.uint64)
+    q = zk.FQ_MODULUS
+    assert not got[0].any()
+    assert np.array_equal(got[1], zk.G1_GENERATOR)
+    assert np.array_equal(got[2][:4], zk.G1_GENERATOR[:4])
+    assert np.array_equal(got[2][4:], oracle.to_mont(q - 2, oracle.FQ))
+    assert np.array_equal(got[3:], pts[3:])

@@ -93,6 +93,49 @@ def test_lagrange_to_extended(zk, oracle, k, e):
     assert np.array_equal(got, ref)
 
 
+@pytest.mark.parametrize("log_ext,m", [(0, 1), (1, 2), (2, 3), (3, 8), (10, 700), (14, 12345), (18, 1 << 18)])
+def test_extended_to_coeff(zk, oracle, log_ext, m):
+    """inverse LDE (ifft on the extended domain, times 7^-i, truncate) vs the oracle"""
+    N = 1 << log_ext
+    ext = oracle.rand_fr(N, 60 + log_ext)
+    w_inv, d = oracle.inv(oracle.omega(log_ext)), inv_n(oracle, log_ext)
+    g_inv = oracle.inv(oracle.to_mont(7))
+    ref = oracle.extended_to_coeff(ext, log_ext, m, w_inv, d, g_inv)
+    got = zk.extended_to_coeff(ext, log_ext, m, w_inv, d, g_inv)
+    assert np.array_equal(got, ref)
+
+
+def test_extended_to_coeff_invalid(zk, oracle):
+    ext = oracle.rand_fr(1 << 10, 1)
+    w_inv, d, g_inv = oracle.inv(oracle.omega(10)), inv_n(oracle, 10), oracle.inv(oracle.to_mont(7))
+    with pytest.raises(zk.ZkGpuError):
+        zk.extended_to_coeff(ext, 10, (1 << 10) + 1, w_inv, d, g_inv)   # m beyond the domain
+    with pytest.raises(zk.ZkGpuError):
+        zk.extended_to_coeff(ext, 10, 16, oracle.inv(oracle.omega(9)), d, g_inv)   # wrong root order
+
+
+def test_lde_inverse_roundtrip_2p24(zk, oracle):
+    """size-independent property at the benchmark size: lagrange 2^24 -> coset
+    extended 2^26 -> coefficients (truncated to 2^24) -> fft gives the values
+    back, and the truncated-away coefficients are all zero"""
+    torch = pytest.importorskip("torch")
+    k, e = 24, 2
+    vals = oracle.rand_fr(1 << k, 424)
+    w, w_ext = oracle.omega(k), oracle.omega(k + e)
+    c = dict(omega_inv=oracle.inv(w), divisor=inv_n(oracle, k), g=oracle.to_mont(7), omega_ext=w_ext)
+    d_vals = torch.from_numpy(vals.view(np.int64)).cuda()
+    d_ext = torch.empty(((1 << (k + e)), 4), dtype=torch.int64, device="cuda")
+    zk.lagrange_to_extended_dev(d_vals, d_ext, k, k + e, c["omega_inv"], c["divisor"], c["g"], c["omega_ext"])
+    d_co = torch.empty(((1 << (k + e)), 4), dtype=torch.int64, device="cuda")
+    zk.extended_to_coeff_dev(d_ext, d_co, k + e, oracle.inv(w_ext), inv_n(oracle, k + e),
+                             oracle.inv(oracle.to_mont(7)))
+    del d_ext
+    assert not d_co[1 << k:].any().item()
+    zk.ntt_dev(d_co[: 1 << k], k, w)
+    torch.cuda.synchronize()
+    assert torch.equal(d_co[: 1 << k], d_vals)
+
+
 def test_edge_inputs(zk, oracle):
     log_n = 14
     n = 1 << log_n

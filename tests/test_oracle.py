@@ -108,6 +108,23 @@ def test_coeff_to_extended_matches_parts(oracle):
     assert ext.shape == (N, 4)
 
 
+def test_extended_to_coeff_inverts_coeff_to_extended(oracle):
+    """extended_to_coeff(coeff_to_extended(a)) == a zero-padded, and the
+    truncation keeps the first m coefficients"""
+    k, e = 7, 2
+    n, N = 1 << k, 1 << (k + e)
+    a = oracle.rand_fr(n, 12)
+    g = oracle.to_mont(7)
+    w_ext = oracle.omega(k + e)
+    ext = oracle.coeff_to_extended(a, k, k + e, g, w_ext)
+    d = oracle.inv(oracle.to_mont(N))
+    back = oracle.extended_to_coeff(ext, k + e, N, oracle.inv(w_ext), d, oracle.inv(g))
+    assert np.array_equal(back[:n], a)
+    assert not back[n:].any()
+    part = oracle.extended_to_coeff(ext, k + e, n + 3, oracle.inv(w_ext), d, oracle.inv(g))
+    assert np.array_equal(part, back[: n + 3])
+
+
 def test_twiddle_lut(oracle):
     # halo2 generate_twiddle_lookup_table(w, k, 10, true): w^i (i<1024) ++ w^(1024 h)
     k = 14

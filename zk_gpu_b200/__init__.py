@@ -21,6 +21,17 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libzkgpu.so")
 
 OK, EINVAL, ENOMEM, ECUDA, ETIMEOUT, EADMIT, ENODEV, EBUSY = range(8)
+# BN254 base field modulus and the G1 generator (1, 2) in Montgomery form
+FQ_MODULUS = 21888242871839275222246405745257275088696311157297823662689037894645226208583
+
+
+def _fq_mont_words(x: int) -> list:
+    m = (x << 256) % FQ_MODULUS
+    return [(m >> (64 * j)) & (2**64 - 1) for j in range(4)]
+
+
+G1_GENERATOR = np.array(_fq_mont_words(1) + _fq_mont_words(2), dtype=np.uint64)
+
 _STATUS = {0: "OK", 1: "EINVAL", 2: "ENOMEM", 3: "ECUDA", 4: "ETIMEOUT", 5: "EADMIT", 6: "ENODEV", 7: "EBUSY"}
 
 _lib = None
@@ -66,6 +77,16 @@ EXPORTS = {
     "zkgpu_lagrange_to_extended_dev": (_i32, [_i32, P, _u32, P, _u32, P, P, P, P, P]),
     "zkgpu_msm_dev": (_i32, [_i32, P, P, _u64, P, P]),
     "zkgpu_ntt_dev_static": (_i32, [_i32, P, _u32, P, P]),
+    "zkgpu_g1_mul_fixed_dev": (_i32, [_i32, P, P, _u64, P, P]),
+    "zkgpu_extended_to_coeff": (_i32, [_i32, P, _u32, P, _u64, P, P, P]),
+    "zkgpu_autotune": (_i32, [_i32, _u32, _u32, _u32, _u32, P]),
+    "zkgpu_tune_set_ntt_plan": (_i32, [_i32, _u32, _u32, P]),
+    "zkgpu_tune_get_ntt_plan": (_i32, [_i32, _u32, P, P]),
+    "zkgpu_tune_set_msm_window": (_i32, [_i32, _u32, _u32]),
+    "zkgpu_tune_get_msm_window": (_i32, [_i32, _u32, P]),
+    "zkgpu_tune_save": (_i32, [_i32, ctypes.c_char_p]),
+    "zkgpu_tune_load": (_i32, [_i32, ctypes.c_char_p, P]),
+    "zkgpu_extended_to_coeff_dev": (_i32, [_i32, P, _u32, P, _u64, P, P, P, P]),
     "zkgpu_ntt_batch_create": (_i32, [_i32, P, _u32, P]),
     "zkgpu_ntt_batch_run": (_i32, [P, P]),
     "zkgpu_ntt_batch_check": (_i32, [P]),
@@ -186,6 +207,18 @@ def lagrange_to_extended(values: np.ndarray, log_n: int, log_ext: int, omega_inv
     return ext
 
 
+def extended_to_coeff(ext: np.ndarray, log_ext: int, m: int, omega_ext_inv, ext_divisor, g_inv,
+                      device: int = 0) -> np.ndarray:
+    """halo2 extended -> coefficients: ifft over 2^log_ext, times g_inv^i,
+    first m coefficients."""
+    e = _arr(ext)
+    out = np.empty((m, 4), np.uint64)
+    _check(lib().zkgpu_extended_to_coeff(device, e.ctypes.data, log_ext, out.ctypes.data, m,
+                                         _el(omega_ext_inv).ctypes.data, _el(ext_divisor).ctypes.data,
+                                         _el(g_inv).ctypes.data), "extended_to_coeff")
+    return out
+
+
 def msm(scalars: np.ndarray, bases: np.ndarray, device: int = 0) -> np.ndarray:
     """Returns the Jacobian sum (12 u64: X, Y, Z), normalised (Z = one) or all-zero."""
     s, b = _arr(scalars), _arr(bases, 8)
@@ -265,6 +298,16 @@ def lagrange_to_extended_dev(values, ext, log_n: int, log_ext: int, omega_inv, d
     _check(lib().zkgpu_lagrange_to_extended_dev(dev, _ptr(values), log_n, _ptr(ext), log_ext, wi.ctypes.data,
                                                 d.ctypes.data, gg.ctypes.data, we.ctypes.data, _stream_ptr(stream)),
            "lagrange_to_extended_dev")
+
+
+def extended_to_coeff_dev(ext, out, log_ext: int, omega_ext_inv, ext_divisor, g_inv, stream=None):
+    """out (m, 4) <- the first m coefficients of ext (2^log_ext, 4) moved off
+    the coset g (g_inv = g^-1); device tensors."""
+    dev = ext.device.index
+    wi, d, gi = _el(omega_ext_inv), _el(ext_divisor), _el(g_inv)
+    _check(lib().zkgpu_extended_to_coeff_dev(dev, _ptr(ext), log_ext, _ptr(out), out.shape[0], wi.ctypes.data,
+                                             d.ctypes.data, gi.ctypes.data, _stream_ptr(stream)),
+           "extended_to_coeff_dev")
 
 
 JOB_COSET, JOB_SCALE = 1, 2
@@ -437,3 +480,60 @@ def msm_dev(scalars, bases, out, stream=None):
     dev = scalars.device.index
     _check(lib().zkgpu_msm_dev(dev, _ptr(scalars), _ptr(bases), scalars.shape[0], _ptr(out), _stream_ptr(stream)),
            "msm_dev")
+
+
+def g1_mul_fixed_dev(scalars, out, base=None, stream=None):
+    """out[i] = scalars[i] * base on the device (affine, Fq Montgomery; base
+    defaults to the generator (1, 2)).  scalars: (n, 4) int64 Fr Montgomery,
+    out: (n, 8) int64."""
+    if base is None:
+        base = G1_GENERATOR
+    b = _arr(base, 8).reshape(-1)
+    dev = scalars.device.index
+    _check(lib().zkgpu_g1_mul_fixed_dev(dev, b.ctypes.data, _ptr(scalars), scalars.shape[0], _ptr(out),
+                                        _stream_ptr(stream)), "g1_mul_fixed_dev")
+
+
+TUNE_NTT, TUNE_MSM, TUNE_NTT_BATCHED = 1, 2, 4
+
+
+def autotune(what: int, log_min: int, log_max: int, device: int = 0, reps: int = 3) -> float:
+    """Time candidate NTT plans / MSM windows for sizes 2^log_min..2^log_max
+    on `device` and install the fastest; returns the device ms spent."""
+    ms = ctypes.c_double()
+    _check(lib().zkgpu_autotune(device, what, log_min, log_max, reps, ctypes.byref(ms)), "autotune")
+    return ms.value
+
+
+def set_ntt_plan(log_n: int, bits, device: int = 0):
+    """Install pass widths for 2^log_n (empty / None: the built-in plan)."""
+    bits = list(bits or [])
+    arr = (ctypes.c_uint32 * max(4, len(bits)))(*(bits + [0] * (4 - len(bits))))
+    _check(lib().zkgpu_tune_set_ntt_plan(device, log_n, len(bits), arr), "tune_set_ntt_plan")
+
+
+def get_ntt_plan(log_n: int, device: int = 0) -> list:
+    npass = ctypes.c_uint32()
+    arr = (ctypes.c_uint32 * 4)()
+    _check(lib().zkgpu_tune_get_ntt_plan(device, log_n, ctypes.byref(npass), arr), "tune_get_ntt_plan")
+    return [int(arr[k]) for k in range(npass.value)]
+
+
+def set_msm_window(log_n: int, c: int, device: int = 0):
+    _check(lib().zkgpu_tune_set_msm_window(device, log_n, c), "tune_set_msm_window")
+
+
+def get_msm_window(log_n: int, device: int = 0) -> int:
+    c = ctypes.c_uint32()
+    _check(lib().zkgpu_tune_get_msm_window(device, log_n, ctypes.byref(c)), "tune_get_msm_window")
+    return c.value
+
+
+def tune_save(path: str, device: int = 0):
+    _check(lib().zkgpu_tune_save(device, path.encode()), "tune_save")
+
+
+def tune_load(path: str, device: int = 0) -> int:
+    n = ctypes.c_uint32()
+    _check(lib().zkgpu_tune_load(device, path.encode(), ctypes.byref(n)), "tune_load")
+    return n.value

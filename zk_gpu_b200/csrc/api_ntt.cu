@@ -116,6 +116,55 @@ int lde_device(int device, const fe* d_values, uint32_t log_n, fe* d_ext, uint32
   return zk::status_of("lde", e);
 }
 
+// Extended -> coefficient form (the inverse of the LDE): ifft over the
+// extended domain, times N^-1 * g_inv^i, first m coefficients to d_out.
+// The scale and the coset powers ride on the ifft's last pass (one table).
+int ext_to_coeff_device(int device, const fe* d_ext, uint32_t log_ext, const hf::Fr& w_inv, const hf::Fr& divisor,
+                        const hf::Fr& g_inv, fe* d_out, uint64_t m, cudaStream_t s) {
+  const size_t N = (size_t)1 << log_ext;
+  cudaError_t e;
+  const zk::NttTables* t = zk::ntt_tables_get(device, w_inv, (int)log_ext, s, &e);
+  if (!t) return zk::status_of("ntt_tables_get", e);
+  const bool tiny = t->plan.npass == 0;  // direct kernel: constant scale only
+  const zk::PowTables* gd = zk::pow_tables_get(device, g_inv, (int)log_ext, s, &e, tiny ? nullptr : &divisor);
+  if (!gd) return zk::status_of("pow_tables_get", e);
+  fe *work = nullptr, *tmp = nullptr;
+  ZK_TRY("cudaMallocAsync(ext_to_coeff work)", cudaMallocAsync((void**)&work, N * sizeof(fe), s));
+  if (t->plan.npass > 1) {
+    e = cudaMallocAsync((void**)&tmp, N * sizeof(fe), s);
+    if (e != cudaSuccess) {
+      cudaFreeAsync(work, s);
+      return zk::status_of("cudaMallocAsync(ext_to_coeff scratch)", e);
+    }
+  }
+  if (tiny) {
+    e = cudaMemcpyAsync(work, d_ext, N * sizeof(fe), cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess) e = zk::ntt_run(*t, work, tmp, nullptr, &divisor, s);
+    if (e == cudaSuccess) e = zk::fr_scale_copy(d_out, work, m, 1, gd, s);
+    zk::count_launches(2);
+  } else {
+    zk::NttFuse f;
+    f.src = d_ext;
+    f.post_tab = gd;
+    e = zk::ntt_run(*t, work, tmp, f, s);
+    zk::count_launches(t->plan.npass);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_out, work, m * sizeof(fe), cudaMemcpyDeviceToDevice, s);
+  }
+  cudaFreeAsync(work, s);
+  if (tmp) cudaFreeAsync(tmp, s);
+  return zk::status_of("ext_to_coeff", e);
+}
+
+int check_etc_args(uint32_t log_ext, const uint64_t* omega_ext_inv, const uint64_t* divisor, const uint64_t* g_inv,
+                   uint64_t m) {
+  if (!omega_ext_inv || !divisor || !g_inv) return ZKGPU_EINVAL;
+  if (log_ext > (uint32_t)zk::NTT_MAX_LOG || m > (1ull << log_ext)) return ZKGPU_EINVAL;
+  hf::Fr w = load_fr(omega_ext_inv), d = load_fr(divisor), g = load_fr(g_inv);
+  if (!hf::is_canonical(w) || !hf::is_canonical(d) || !hf::is_canonical(g)) return ZKGPU_EINVAL;
+  if (!hf::is_primitive_root(w, log_ext)) return ZKGPU_EINVAL;
+  return ZKGPU_OK;
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -249,6 +298,53 @@ extern "C" int zkgpu_lagrange_to_extended_dev(int device, const uint64_t* d_valu
   if (st) return st;
   return lde_device(device, reinterpret_cast<const fe*>(d_values), log_n, reinterpret_cast<fe*>(d_ext), log_ext,
                     load_fr(omega_inv), load_fr(divisor), load_fr(g), load_fr(omega_ext), (cudaStream_t)stream);
+}
+
+extern "C" int zkgpu_extended_to_coeff(int device, const uint64_t* ext, uint32_t log_ext, uint64_t* out, uint64_t m,
+                                       const uint64_t omega_ext_inv[4], const uint64_t ext_divisor[4],
+                                       const uint64_t g_inv[4]) {
+  if (!ext || (m && !out)) return ZKGPU_EINVAL;
+  int st = check_etc_args(log_ext, omega_ext_inv, ext_divisor, g_inv, m);
+  if (st) return st;
+  if (m == 0) return ZKGPU_OK;
+  cudaStream_t s;
+  st = zk::bind_device(device, &s);
+  if (st) return st;
+  const size_t N = (size_t)1 << log_ext;
+  fe *d_ext = nullptr, *d_out = nullptr;
+  ZK_TRY("cudaMallocAsync(ext_to_coeff in)", cudaMallocAsync((void**)&d_ext, N * sizeof(fe), s));
+  cudaError_t e = cudaMallocAsync((void**)&d_out, m * sizeof(fe), s);
+  if (e != cudaSuccess) {
+    cudaFreeAsync(d_ext, s);
+    return zk::status_of("cudaMallocAsync(ext_to_coeff out)", e);
+  }
+  e = cudaMemcpyAsync(d_ext, ext, N * sizeof(fe), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) {
+    st = ext_to_coeff_device(device, d_ext, log_ext, load_fr(omega_ext_inv), load_fr(ext_divisor), load_fr(g_inv),
+                             d_out, m, s);
+    if (st == ZKGPU_OK) e = cudaMemcpyAsync(out, d_out, m * sizeof(fe), cudaMemcpyDeviceToHost, s);
+  }
+  cudaFreeAsync(d_ext, s);
+  cudaFreeAsync(d_out, s);
+  cudaError_t e2 = cudaStreamSynchronize(s);
+  if (st) return st;
+  if (e != cudaSuccess) return zk::status_of("ext_to_coeff copy", e);
+  return zk::status_of("ext_to_coeff sync", e2);
+}
+
+extern "C" int zkgpu_extended_to_coeff_dev(int device, const uint64_t* d_ext, uint32_t log_ext, uint64_t* d_out,
+                                           uint64_t m, const uint64_t omega_ext_inv[4], const uint64_t ext_divisor[4],
+                                           const uint64_t g_inv[4], void* stream) {
+  if (!d_ext || (m && !d_out)) return ZKGPU_EINVAL;
+  int st = check_etc_args(log_ext, omega_ext_inv, ext_divisor, g_inv, m);
+  if (st) return st;
+  if (m == 0) return ZKGPU_OK;
+  cudaStream_t own;
+  st = zk::bind_device(device, &own);
+  if (st) return st;
+  return ext_to_coeff_device(device, reinterpret_cast<const fe*>(d_ext), log_ext, load_fr(omega_ext_inv),
+                             load_fr(ext_divisor), load_fr(g_inv), reinterpret_cast<fe*>(d_out), m,
+                             (cudaStream_t)stream);
 }
 
 // ===========================================================================

@@ -14,6 +14,10 @@ MsmPlan make_msm_plan(uint64_t n, int c_override) {
   int c = lg - 4;
   if (c < 4) c = 4;
   if (c > 16) c = 16;
+  if (c_override == 0) {  // the autotuner's choice for this device and size, if any
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) c_override = tuned_msm_window(dev, lg);
+  }
   if (c_override >= 3 && c_override <= 20) c = c_override;
   p.c = c;
   p.windows = (254 + c - 1) / c;

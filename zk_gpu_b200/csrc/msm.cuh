@@ -28,7 +28,11 @@ struct MsmPlan {
   uint32_t buckets = 0;  // per window, 2^(c-1)
   uint32_t seg_len = 0;  // buckets per reduction segment
 };
+// c_override = 0: the autotuner's window for the current device, else
+// clamp(ceil(log2 n) - 4, 4, 16).
 MsmPlan make_msm_plan(uint64_t n, int c_override = 0);
+// The window installed by the autotuner for (device, log2 n), or 0.
+int tuned_msm_window(int device, int log_n);
 
 // Enqueue the MSM on `s`; d_out receives the Jacobian sum (X, Y, Z: 12 u64,
 // not normalised; identity = Z 0).  Scratch comes from the stream pool.

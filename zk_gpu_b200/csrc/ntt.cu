@@ -492,10 +492,17 @@ struct Key {
   int dev;
   int log_n;
   uint64_t w[4];
+  uint32_t plan;  // pass widths, 6 bits each
   bool operator<(const Key& o) const {
-    return std::tie(dev, log_n, w[0], w[1], w[2], w[3]) < std::tie(o.dev, o.log_n, o.w[0], o.w[1], o.w[2], o.w[3]);
+    return std::tie(dev, log_n, w[0], w[1], w[2], w[3], plan) <
+           std::tie(o.dev, o.log_n, o.w[0], o.w[1], o.w[2], o.w[3], o.plan);
   }
 };
+uint32_t plan_code(const NttPlan& p) {
+  uint32_t c = (uint32_t)p.npass;
+  for (int k = 0; k < NTT_MAX_PASS; k++) c = (c << 6) | (uint32_t)p.bits[k];
+  return c;
+}
 std::mutex g_mu;
 std::map<Key, std::unique_ptr<NttTables>> g_cache;
 }  // namespace
@@ -590,8 +597,45 @@ cudaError_t ntt_tables_fill(NttTables* t, const host::Fr& omega, int log_n, fe* 
   return cudaGetLastError();
 }
 
+bool ntt_plan_valid(const NttPlan& p) {
+  if (p.log_n < 0 || p.log_n > NTT_MAX_LOG) return false;
+  if (p.log_n <= 2) return p.npass == 0;
+  if (p.npass < 1 || p.npass > NTT_MAX_PASS) return false;
+  if (p.npass == 1) return p.bits[0] == p.log_n && p.log_n <= 11;
+  int sum = 0;
+  for (int k = 0; k < p.npass; k++) {
+    if (p.bits[k] < 3 || p.bits[k] > 11) return false;
+    sum += p.bits[k];
+  }
+  for (int k = p.npass; k < NTT_MAX_PASS; k++)
+    if (p.bits[k] != 0) return false;
+  return sum == p.log_n;
+}
+
+cudaError_t ntt_tables_build(NttTables* t, const NttPlan& plan, const host::Fr& omega, cudaStream_t s) {
+  if (!ntt_plan_valid(plan)) return cudaErrorInvalidValue;
+  *t = NttTables{};
+  t->plan = plan;
+  t->omega = omega;
+  cudaError_t e = build_tables(t, s);
+  if (e != cudaSuccess) ntt_tables_release(t);
+  return e;
+}
+
+void ntt_tables_release(NttTables* t) {
+  for (int k = 0; k < NTT_MAX_PASS; k++) {
+    if (t->inner[k]) cudaFree(t->inner[k]);
+    if (t->twist[k]) cudaFree(t->twist[k]);
+    t->inner[k] = t->twist[k] = nullptr;
+  }
+  t->bytes = 0;
+}
+
 const NttTables* ntt_tables_get(int device, const host::Fr& omega, int log_n, cudaStream_t s, cudaError_t* err) {
-  Key key{device, log_n, {omega.v[0], omega.v[1], omega.v[2], omega.v[3]}};
+  // the plan is the autotuner's choice for this device and size, if any;
+  // tables of a plan stay cached after the choice changes (work may still use them)
+  const NttPlan plan = tuned_ntt_plan(device, log_n);
+  Key key{device, log_n, {omega.v[0], omega.v[1], omega.v[2], omega.v[3]}, plan_code(plan)};
   std::lock_guard<std::mutex> lk(g_mu);
   auto it = g_cache.find(key);
   if (it != g_cache.end()) {
@@ -599,14 +643,8 @@ const NttTables* ntt_tables_get(int device, const host::Fr& omega, int log_n, cu
     return it->second.get();
   }
   auto t = std::make_unique<NttTables>();
-  t->plan = make_ntt_plan(log_n);
-  t->omega = omega;
-  cudaError_t e = build_tables(t.get(), s);
+  cudaError_t e = ntt_tables_build(t.get(), plan, omega, s);
   if (e != cudaSuccess) {
-    for (int k = 0; k < NTT_MAX_PASS; k++) {
-      if (t->inner[k]) cudaFree(t->inner[k]);
-      if (t->twist[k]) cudaFree(t->twist[k]);
-    }
     *err = e;
     return nullptr;
   }

@@ -33,6 +33,11 @@ struct NttPlan {
   int bits[NTT_MAX_PASS] = {0, 0, 0, 0};
 };
 NttPlan make_ntt_plan(int log_n);
+// Supported plans: log_n <= 2 direct (no passes); one pass of log_n <= 11
+// bits; or 2..4 passes of 3..11 bits summing to log_n.
+bool ntt_plan_valid(const NttPlan& p);
+// The plan the autotuner chose for (device, log_n), else make_ntt_plan.
+NttPlan tuned_ntt_plan(int device, int log_n);
 
 // Device tables for one (omega, log_n): per pass the inner roots
 // w_m^e (e < m/2) and, for non-final passes, the twist table [k * J + j].
@@ -55,6 +60,10 @@ struct PowTables {
 // Cached tables for (device, omega, log_n); thread-safe.  Returns nullptr and
 // sets *err on failure.  The cache owns the memory.
 const NttTables* ntt_tables_get(int device, const host::Fr& omega, int log_n, cudaStream_t s, cudaError_t* err);
+// Uncached tables for an explicit plan (the autotuner's trials); free with
+// ntt_tables_release after the work using them has finished.
+cudaError_t ntt_tables_build(NttTables* t, const NttPlan& plan, const host::Fr& omega, cudaStream_t s);
+void ntt_tables_release(NttTables* t);
 // Tables for (omega, log_n) written into caller-provided device memory of
 // `cap` elements (no allocation); ntt_tables_elems gives the size needed.
 size_t ntt_tables_elems(int log_n);
