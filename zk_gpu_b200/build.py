@@ -23,6 +23,12 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
          "--expt-relaxed-constexpr", "-I", INCLUDE, "-I", CSRC]
+# extra nvcc flags, e.g. ZKGPU_NVCC_EXTRA="-DZK_NTT_MIN_BLOCKS=1" (CTAs per SM
+# the NTT pass kernels are compiled for); BUILD_DIR / LIB may be redirected
+# with ZKGPU_BUILD_DIR / ZKGPU_LIB_OUT to keep such a variant apart
+FLAGS += os.environ.get("ZKGPU_NVCC_EXTRA", "").split()
+BUILD = os.environ.get("ZKGPU_BUILD_DIR", BUILD)
+LIB = os.environ.get("ZKGPU_LIB_OUT", LIB)
 
 
 def _headers_mtime() -> float:

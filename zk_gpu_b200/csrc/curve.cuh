@@ -9,8 +9,8 @@
 // not recognised as zero afterwards).  Affine inputs use (0, 0) for the
 // identity (cuda/bn256.h:15-20).
 //
-// Arithmetic form: every coordinate is kept in the R' = 2^261 Montgomery
-// form of the radix-2^29 product (mul_r29: R'-form x R'-form -> R'-form),
+// Arithmetic form: every coordinate is kept in the R' = 2^260 Montgomery
+// form of the FP64 52-bit-limb product (mul_rp: R'-form x R'-form -> R'-form),
 // lazily reduced in [0, 2q); values are made canonical only where they are
 // compared with zero.  to_rprime / from_rprime convert from / to the
 // R = 2^256 form used in memory by the API (bit-identical to halo2curves).
@@ -29,8 +29,8 @@ struct aff_t {
 };
 
 // ---- lazy R'-form Fq helpers --------------------------------------------
-__device__ __forceinline__ void qmul(uint32_t r[8], const uint32_t a[8], const uint32_t b[8]) { mul_r29<P_q>(r, a, b); }
-__device__ __forceinline__ void qsqr(uint32_t r[8], const uint32_t a[8]) { mul_r29<P_q>(r, a, a); }
+__device__ __forceinline__ void qmul(uint32_t r[8], const uint32_t a[8], const uint32_t b[8]) { mul_rp<P_q>(r, a, b); }
+__device__ __forceinline__ void qsqr(uint32_t r[8], const uint32_t a[8]) { mul_rp<P_q>(r, a, a); }
 __device__ __forceinline__ void qadd(uint32_t r[8], const uint32_t a[8], const uint32_t b[8]) { add_lazy<P_q>(r, a, b); }
 __device__ __forceinline__ void qsub(uint32_t r[8], const uint32_t a[8], const uint32_t b[8]) { sub_lazy<P_q>(r, a, b); }
 __device__ __forceinline__ void qdbl(uint32_t r[8], const uint32_t a[8]) { add_lazy<P_q>(r, a, a); }
@@ -39,18 +39,18 @@ __device__ __forceinline__ bool qzero(const uint32_t a[8]) {
   reduce_once<P_q>(c, a);
   return is_zero(c);
 }
-// x (R form, x * 2^256) -> x * 2^261, canonical: multiply by 2^266 mod q
+// x (R form, x * 2^256) -> x * 2^260, canonical: multiply by 2^264 mod q
 __device__ __forceinline__ void to_rprime(uint32_t r[8], const uint32_t a[8]) {
-  const uint32_t k[8] = {0x13349ca1u, 0xb34bb095u, 0xf028f972u, 0x1e880124u,
-                         0xa6092b95u, 0xe56cdd25u, 0xdce9ed32u, 0x05800320u};
-  mul_r29<P_q>(r, a, k);
+  const uint32_t k[8] = {0xfaec667au, 0xfbdb0f2au, 0x9626b0ffu, 0xad825aedu,
+                         0x09e2a0fcu, 0x276f48b7u, 0xef86e357u, 0x0d791464u};
+  mul_rp<P_q>(r, a, k);
   reduce_once<P_q>(r, r);
 }
-// x * 2^261 (lazy) -> x * 2^256, canonical: multiply by 2^256 mod q
+// x * 2^260 (lazy) -> x * 2^256, canonical: multiply by 2^256 mod q
 __device__ __forceinline__ void from_rprime(uint32_t r[8], const uint32_t a[8]) {
   uint32_t one_r[8];
   set_one<P_q>(one_r);  // the integer 2^256 mod q
-  mul_r29<P_q>(r, a, one_r);
+  mul_rp<P_q>(r, a, one_r);
   reduce_once<P_q>(r, r);
 }
 
@@ -70,8 +70,8 @@ __device__ __forceinline__ void xyzz_from_aff(xyzz_t& r, const aff_t& q) {
   }
   cpy(r.x, q.x);
   cpy(r.y, q.y);
-  set_one_r29<P_q>(r.zz);
-  set_one_r29<P_q>(r.zzz);
+  set_one_rp<P_q>(r.zz);
+  set_one_rp<P_q>(r.zzz);
 }
 
 // r = 2p  (dbl-2008-s-1, a = 0).  The identity doubles to itself (ZZ stays 0).

@@ -54,7 +54,7 @@ __global__ void modmul_rate_kernel(uint32_t* sink, uint32_t iters, uint32_t seed
   }
   for (uint32_t it = 0; it < iters; it++) {
 #pragma unroll
-    for (int k = 0; k < 4; k++) mul_r29<FrP>(x[k], x[k], y);
+    for (int k = 0; k < 4; k++) mul_rp<FrP>(x[k], x[k], y);
   }
   uint32_t acc = 0;
 #pragma unroll

@@ -34,9 +34,12 @@ struct FrP {
   // R mod p (Montgomery one)
   static constexpr uint32_t O0 = 0x4ffffffbu, O1 = 0xac96341cu, O2 = 0x9f60cd29u, O3 = 0x36fc7695u,
                             O4 = 0x7879462eu, O5 = 0x666ea36fu, O6 = 0x9a07df2fu, O7 = 0x0e0a77c1u;
-  // 2^261 mod p (the one of the R' = 2^261 form used by mul_r29)
+  // 2^261 mod p (the one of the 2^261 form of the IMAD product mul_r29)
   static constexpr uint32_t Q0 = 0x8fffff57u, Q1 = 0x2fd4e156u, Q2 = 0xa494b01au, Q3 = 0x75bba827u,
                             Q4 = 0x819caa80u, Q5 = 0x5301fa84u, Q6 = 0x563d4475u, Q7 = 0x0dc83629u;
+  // 2^260 mod p (the one of the R' = 2^260 form used by mul_rp)
+  static constexpr uint32_t D0 = 0x3fffffacu, D1 = 0xb9db6b75u, D2 = 0x0f271055u, D3 = 0xcef7c838u,
+                            D4 = 0x818f016eu, D5 = 0x85a9201du, D6 = 0x1bb7724fu, D7 = 0x1f16424eu;
 };
 struct FqP {
   static constexpr uint32_t P0 = 0xd87cfd47u, P1 = 0x3c208c16u, P2 = 0x6871ca8du, P3 = 0x97816a91u,
@@ -46,6 +49,8 @@ struct FqP {
                             O4 = 0x7879462cu, O5 = 0x666ea36fu, O6 = 0x9a07df2fu, O7 = 0x0e0a77c1u;
   static constexpr uint32_t Q0 = 0x157ccc21u, Q1 = 0x4e8384ebu, Q2 = 0x0ce148c3u, Q3 = 0xfb90a602u,
                             Q4 = 0x819caa36u, Q5 = 0x5301fa84u, Q6 = 0x563d4475u, Q7 = 0x0dc83629u;
+  static constexpr uint32_t D0 = 0xf6fce4b4u, D1 = 0x45520880u, D2 = 0xbaa989a8u, D3 = 0x49890849u,
+                            D4 = 0x818f014au, D5 = 0x85a9201du, D6 = 0x1bb7724fu, D7 = 0x1f16424eu;
 };
 
 #define ZK_P_OPS(P) "n"(P::INV), "n"(P::P0), "n"(P::P1), "n"(P::P2), "n"(P::P3), "n"(P::P4), "n"(P::P5), "n"(P::P6), "n"(P::P7)
@@ -473,6 +478,168 @@ __device__ __forceinline__ void pow_u64_r29(uint32_t r[8], const uint32_t a[8], 
     if (e & 1) mul_r29<P>(acc, acc, base);
     e >>= 1;
     if (e) mul_r29<P>(base, base, base);
+  }
+  reduce_once<P>(r, acc);
+}
+
+// ---- FP64 product: 5 limbs of 52 bits in doubles, R' = 2^260 --------------
+// The hot-path product.  Limbs are exact integers < 2^52 held in doubles;
+// each 52 x 52-bit partial product is split exactly into its high and low
+// 52-bit halves by two fused multiply-adds rounded toward zero:
+//   h = fma_rz(a, b, 2^104)             = 2^104 + floor(ab / 2^52) 2^52
+//   l = fma_rz(a, b, 2^104 + 2^52 - h)  = 2^52  + (ab mod 2^52)
+// Every value involved is exactly representable (the subtraction
+// 2^104 + 2^52 - h too), so nothing is rounded.  The IEEE bit patterns of h
+// and l are integers with a constant bias: bits(h) - bits(2^104) =
+// floor(ab / 2^52) and bits(l) - bits(2^52) = ab mod 2^52.  They are summed
+// per column (product scanning) in 64-bit integers, the biases removed once
+// per column, and the Montgomery quotient digit m_k = t_k (-p^-1) mod 2^52
+// comes from an integer multiply; its products m_k p_j are split the same
+// way.  The result is a b 2^-260 mod p, lazily reduced: inputs < 2p give an
+// output < 2p (4p^2 / 2^260 < p).  This moves the 256-bit product from the
+// 32-bit IMAD pipe (mul29_cols: 81 + 81 word products as lo/hi pairs) to
+// the FP64 pipe (50 + 50 DFMA, 50 exact DADD) with the column sums on the
+// integer ALU; measured 1.4x the product rate of mul29_cols on B200.  The
+// method is the one published by Emmart, Zheng and Weems, "Faster Modular
+// Exponentiation Using Double Precision Floating Point Arithmetic on the
+// GPU" (ARITH 2018).
+constexpr uint64_t M52 = (1ull << 52) - 1;
+constexpr double D2P52 = 4503599627370496.0;                      // 2^52
+constexpr double D2P104 = 20282409603651670423947251286016.0;     // 2^104
+constexpr double D2P104_52 = 20282409603651674927546878656512.0;  // 2^104 + 2^52
+constexpr uint64_t BITS_2P52 = 0x4330000000000000ull;
+constexpr uint64_t BITS_2P104 = 0x4670000000000000ull;
+
+template <class P>
+__host__ __device__ constexpr uint64_t pword64(int k) {
+  return k == 0   ? ((uint64_t)P::P1 << 32 | P::P0)
+         : k == 1 ? ((uint64_t)P::P3 << 32 | P::P2)
+         : k == 2 ? ((uint64_t)P::P5 << 32 | P::P4)
+                  : ((uint64_t)P::P7 << 32 | P::P6);
+}
+// limb j (52 bits) of the modulus, as a double
+template <class P>
+__host__ __device__ constexpr double p52(int j) {
+  return (double)(j == 0   ? (pword64<P>(0) & M52)
+                  : j == 1 ? ((pword64<P>(0) >> 52 | pword64<P>(1) << 12) & M52)
+                  : j == 2 ? ((pword64<P>(1) >> 40 | pword64<P>(2) << 24) & M52)
+                  : j == 3 ? ((pword64<P>(2) >> 28 | pword64<P>(3) << 36) & M52)
+                           : (pword64<P>(3) >> 16));
+}
+// -p^-1 mod 2^52 (Newton iteration on the low word)
+template <class P>
+__host__ __device__ constexpr uint64_t pinv52() {
+  uint64_t x = 1;
+  for (int i = 0; i < 7; i++) x *= 2 - pword64<P>(0) * x;
+  return (0 - x) & M52;
+}
+
+__device__ __forceinline__ double dbl_of_limb(uint64_t v) {  // v < 2^52 -> (double)v, exactly
+  return __longlong_as_double((long long)(v | BITS_2P52)) - D2P52;
+}
+__device__ __forceinline__ uint64_t bits_of(double x) { return (uint64_t)__double_as_longlong(x); }
+
+__device__ __forceinline__ void split52(double l[5], const uint32_t a[8]) {
+  const uint64_t x0 = (uint64_t)a[1] << 32 | a[0], x1 = (uint64_t)a[3] << 32 | a[2];
+  const uint64_t x2 = (uint64_t)a[5] << 32 | a[4], x3 = (uint64_t)a[7] << 32 | a[6];
+  l[0] = dbl_of_limb(x0 & M52);
+  l[1] = dbl_of_limb((x0 >> 52 | x1 << 12) & M52);
+  l[2] = dbl_of_limb((x1 >> 40 | x2 << 24) & M52);
+  l[3] = dbl_of_limb((x2 >> 28 | x3 << 36) & M52);
+  l[4] = dbl_of_limb(x3 >> 16);
+}
+__device__ __forceinline__ void pack52(uint32_t r[8], const uint64_t l[5]) {
+  const uint64_t x0 = l[0] | l[1] << 52, x1 = l[1] >> 12 | l[2] << 40;
+  const uint64_t x2 = l[2] >> 24 | l[3] << 28, x3 = l[3] >> 36 | l[4] << 16;
+  r[0] = (uint32_t)x0; r[1] = (uint32_t)(x0 >> 32); r[2] = (uint32_t)x1; r[3] = (uint32_t)(x1 >> 32);
+  r[4] = (uint32_t)x2; r[5] = (uint32_t)(x2 >> 32); r[6] = (uint32_t)x3; r[7] = (uint32_t)(x3 >> 32);
+}
+
+// index pairs (j, i), 0 <= i, j < 5, with i + j = k
+__host__ __device__ constexpr int npairs5(int k) { return k < 0 || k > 8 ? 0 : (k <= 4 ? k + 1 : 9 - k); }
+// quotient terms m_j p_i with j + i = k (m_k p_0 included for k < 5)
+__host__ __device__ constexpr int nquot5(int k) { return k < 0 ? 0 : (k < 5 ? k + 1 : npairs5(k)); }
+
+// a * b * 2^-260 mod p as 5 normalised 52-bit limbs (a, b < 2p as limbs)
+template <class P>
+__device__ __forceinline__ void mul52_cols(uint64_t rl[5], const double a[5], const double b[5]) {
+  double m[5];
+  uint64_t cur = 0, nxt = 0;
+#pragma unroll
+  for (int k = 0; k < 10; k++) {
+#pragma unroll
+    for (int j = 0; j < 5; j++) {
+      const int i = k - j;
+      if (i >= 0 && i < 5) {
+        const double h = __fma_rz(a[j], b[i], D2P104);
+        const double l = __fma_rz(a[j], b[i], D2P104_52 - h);
+        cur += bits_of(l);
+        nxt += bits_of(h);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 5; j++) {
+      const int i = k - j;
+      if (j < k && i >= 0 && i < 5) {
+        const double h = __fma_rz(m[j], p52<P>(i), D2P104);
+        const double l = __fma_rz(m[j], p52<P>(i), D2P104_52 - h);
+        cur += bits_of(l);
+        nxt += bits_of(h);
+      }
+    }
+    // biases: this column's low halves so far, and the high halves the
+    // previous column passed on (they arrived in `cur` with the carry)
+    const uint64_t nlo = (uint64_t)(npairs5(k) + (k < 5 ? k : npairs5(k)));
+    const uint64_t nhi = (uint64_t)(npairs5(k - 1) + nquot5(k - 1));
+    cur -= nlo * BITS_2P52 + nhi * BITS_2P104;
+    if (k < 5) {
+      m[k] = dbl_of_limb(((cur & M52) * pinv52<P>()) & M52);
+      const double h = __fma_rz(m[k], p52<P>(0), D2P104);
+      const double l = __fma_rz(m[k], p52<P>(0), D2P104_52 - h);
+      cur += bits_of(l) - BITS_2P52;  // now a multiple of 2^52
+      nxt += bits_of(h);
+    } else {
+      rl[k - 5] = cur & M52;
+    }
+    cur = nxt + (cur >> 52);
+    nxt = 0;
+  }
+}
+
+// 8-word interface: r = a * b' * 2^-260 (b' in R' form), lazy (< 2p)
+template <class P>
+__device__ __forceinline__ void mul_rp(uint32_t r[8], const uint32_t a[8], const uint32_t b[8]) {
+  double al[5], bl[5];
+  uint64_t rl[5];
+  split52(al, a);
+  split52(bl, b);
+  mul52_cols<P>(rl, al, bl);
+  pack52(r, rl);
+}
+// a (8 words) times a pre-split R'-form constant
+template <class P>
+__device__ __forceinline__ void mul_rp_pre(uint32_t r[8], const uint32_t a[8], const double bl[5]) {
+  double al[5];
+  uint64_t rl[5];
+  split52(al, a);
+  mul52_cols<P>(rl, al, bl);
+  pack52(r, rl);
+}
+template <class P>
+__device__ __forceinline__ void set_one_rp(uint32_t r[8]) {
+  r[0] = P::D0; r[1] = P::D1; r[2] = P::D2; r[3] = P::D3;
+  r[4] = P::D4; r[5] = P::D5; r[6] = P::D6; r[7] = P::D7;
+}
+// a^e with a and the result in R' form (canonical)
+template <class P>
+__device__ __forceinline__ void pow_u64_rp(uint32_t r[8], const uint32_t a[8], uint64_t e) {
+  uint32_t acc[8], base[8];
+  set_one_rp<P>(acc);
+  cpy(base, a);
+  while (e) {
+    if (e & 1) mul_rp<P>(acc, acc, base);
+    e >>= 1;
+    if (e) mul_rp<P>(base, base, base);
   }
   reduce_once<P>(r, acc);
 }

@@ -9,7 +9,7 @@
 // 1 <= d < 16) is built once per call by 64 threads, normalised to affine;
 // each scalar then costs at most 64 mixed additions (XYZZ madd) and one field
 // inversion (Fermat, a^(q-2)) to return to affine.  All arithmetic is the
-// radix-2^29 R'-form product of field.cuh; outputs are canonical R-form
+// R'-form product (mul_rp) of field.cuh; outputs are canonical R-form
 // (Montgomery, 2^256) affine points, (0, 0) for the identity.
 #include <cuda_runtime.h>
 
@@ -20,10 +20,10 @@ namespace zk {
 namespace {
 
 // a^(q-2) = a^-1 for a != 0, R' form in and out (lazy in, canonical out)
-__device__ void fq_inv_r29(uint32_t r[8], const uint32_t a[8]) {
+__device__ void fq_inv_rp(uint32_t r[8], const uint32_t a[8]) {
   const uint32_t e[8] = {FqP::P0 - 2u, FqP::P1, FqP::P2, FqP::P3, FqP::P4, FqP::P5, FqP::P6, FqP::P7};
   uint32_t acc[8];
-  set_one_r29<FqP>(acc);
+  set_one_rp<FqP>(acc);
   for (int w = 7; w >= 0; w--) {
     for (int b = 31; b >= 0; b--) {
       qsqr(acc, acc);
@@ -42,7 +42,7 @@ __device__ void xyzz_to_affine_rp(aff_t& o, const xyzz_t& p) {
   }
   uint32_t t[8], inv[8], izz[8], izzz[8];
   qmul(t, p.zz, p.zzz);
-  fq_inv_r29(inv, t);       // 1 / (ZZ ZZZ)
+  fq_inv_rp(inv, t);       // 1 / (ZZ ZZZ)
   qmul(izz, inv, p.zzz);    // 1 / ZZ
   qmul(izzz, inv, p.zz);    // 1 / ZZZ
   qmul(o.x, p.x, izz);

@@ -61,10 +61,10 @@ __device__ __forceinline__ void ld_smem_fe(uint32_t r[8], const uint32_t* plane0
 #pragma unroll
   for (int k = 0; k < 8; k++) r[k] = plane0[k * plane_stride + a];
 }
-// a twiddle stored as 9 pre-split 29-bit limb planes
-__device__ __forceinline__ void ld_smem_tw(uint32_t r[9], const uint32_t* plane0, uint32_t plane_stride, uint32_t a) {
+// a twiddle stored pre-split as 5 planes of 52-bit limbs (doubles)
+__device__ __forceinline__ void ld_smem_tw(double r[5], const double* plane0, uint32_t plane_stride, uint32_t a) {
 #pragma unroll
-  for (int k = 0; k < 9; k++) r[k] = plane0[k * plane_stride + a];
+  for (int k = 0; k < 5; k++) r[k] = plane0[k * plane_stride + a];
 }
 __device__ __forceinline__ void st_smem_fe(uint32_t* plane0, uint32_t plane_stride, uint32_t a, const uint32_t r[8]) {
 #pragma unroll
@@ -72,9 +72,9 @@ __device__ __forceinline__ void st_smem_fe(uint32_t* plane0, uint32_t plane_stri
 }
 
 // One round: registers hold i(r) = ins3<LO>(q, r); perform the DIF stages
-// with butterfly bits HI-1 .. LO.  tws: inner roots w_m^e (e < m/2), 8 planes.
+// with butterfly bits HI-1 .. LO.  tws: inner roots w_m^e (e < m/2), 5 planes.
 template <int B, int LO, int HI>
-__device__ __forceinline__ void ntt_round(uint32_t x[8][8], uint32_t q, const uint32_t* tws) {
+__device__ __forceinline__ void ntt_round(uint32_t x[8][8], uint32_t q, const double* tws) {
   constexpr uint32_t HALF = 1u << (B - 1);
 #pragma unroll
   for (int b = HI - 1; b >= LO; b--) {
@@ -93,15 +93,15 @@ __device__ __forceinline__ void ntt_round(uint32_t x[8][8], uint32_t q, const ui
 #pragma unroll
           for (int k = 0; k < 8; k++) x[r2][k] = t[k];
         } else {
-          uint32_t w[9];
+          double w[5];
           ld_smem_tw(w, tws, HALF, e);
-          mul_r29_pre<P_r>(x[r2], t, w);
+          mul_rp_pre<P_r>(x[r2], t, w);
         }
       } else {
         const uint32_t e = ((q & ((1u << LO) - 1u)) | ((uint32_t)(r & ((1 << rb) - 1)) << LO)) << (B - 1 - b);
-        uint32_t w[9];
+        double w[5];
         ld_smem_tw(w, tws, HALF, e);
-        mul_r29_pre<P_r>(x[r2], t, w);
+        mul_rp_pre<P_r>(x[r2], t, w);
       }
     }
   }
@@ -124,7 +124,7 @@ __device__ __forceinline__ void ntt_exchange(uint32_t x[8][8], uint32_t q, uint3
 
 template <int B, int HI>
 __device__ __forceinline__ void ntt_rounds(uint32_t x[8][8], uint32_t q, uint32_t gbase, uint32_t* sm,
-                                           uint32_t plane_stride, const uint32_t* tws, bool active) {
+                                           uint32_t plane_stride, const double* tws, bool active) {
   constexpr int LO = HI - 3 > 0 ? HI - 3 : 0;
   ntt_round<B, LO, HI>(x, q, tws);
   if constexpr (LO > 0) {
@@ -149,18 +149,19 @@ __device__ __forceinline__ void ntt_pass_tile(const PassParams& p, uint64_t tile
   constexpr uint32_t T = M / 8;  // threads per column
   const uint32_t G = p.G;
   const uint32_t plane_stride = G * M;
-  uint32_t* tws = smem + 8 * plane_stride;
+  double* tws = reinterpret_cast<double*>(smem + 8 * plane_stride);  // 8-byte aligned: 32 G M bytes in
 
   const uint32_t tid = threadIdx.x;
   const uint32_t g = tid / T, q = tid % T;
   const bool active = !BATCH || g < G;
 
   for (uint32_t e = tid; e < M / 2; e += blockDim.x) {
-    uint32_t w[8], wl[9];
+    uint32_t w[8];
+    double wl[5];
     ld_fe_nc(w, p.inner + e);
-    split29(wl, w);  // stored pre-split: 9 limb planes
+    split52(wl, w);  // stored pre-split: 5 limb planes
 #pragma unroll
-    for (int k = 0; k < 9; k++) tws[k * (M / 2) + e] = wl[k];
+    for (int k = 0; k < 5; k++) tws[k * (M / 2) + e] = wl[k];
   }
 
   // element indices are < 2^28: 32-bit arithmetic, powers of two as shifts
@@ -208,8 +209,8 @@ __device__ __forceinline__ void ntt_pass_tile(const PassParams& p, uint64_t tile
       uint32_t a[8], b[8];
       ld_fe_nc(a, p.pre_lo + (xi & mask));
       ld_fe_nc(b, p.pre_hi + (xi >> p.pre_shift));
-      mul_r29<P_r>(a, a, b);
-      mul_r29<P_r>(x[r], x[r], a);
+      mul_rp<P_r>(a, a, b);
+      mul_rp<P_r>(x[r], x[r], a);
     }
   }
   __syncthreads();
@@ -225,7 +226,7 @@ __device__ __forceinline__ void ntt_pass_tile(const PassParams& p, uint64_t tile
       uint32_t w[8];
       const uint32_t kj = (k << p.log_J) + col;
       ld_fe_nc(w, p.twist + kj);
-      mul_r29<P_r>(x[r], x[r], w);
+      mul_rp<P_r>(x[r], x[r], w);
       st_fe(p.out + (((o << B) << p.log_J) + kj), x[r]);
     }
   } else {
@@ -255,11 +256,11 @@ __device__ __forceinline__ void ntt_pass_tile(const PassParams& p, uint64_t tile
         uint32_t a[8], b[8];
         ld_fe_nc(a, p.post_lo + (kout & ((1u << p.post_shift) - 1u)));
         ld_fe_nc(b, p.post_hi + (kout >> p.post_shift));
-        mul_r29<P_r>(a, a, b);
-        mul_r29<P_r>(v, x[r], a);
+        mul_rp<P_r>(a, a, b);
+        mul_rp<P_r>(v, x[r], a);
         reduce_once<P_r>(v, v);
       } else if (p.has_post) {
-        mul_r29<P_r>(v, x[r], p.post.w);
+        mul_rp<P_r>(v, x[r], p.post.w);
         reduce_once<P_r>(v, v);
       } else {
         reduce_once<P_r>(v, x[r]);
@@ -271,7 +272,7 @@ __device__ __forceinline__ void ntt_pass_tile(const PassParams& p, uint64_t tile
 
 template <int B>
 __global__ void __launch_bounds__(256, ZK_NTT_MIN_BLOCKS) ntt_pass_kernel(const PassParams p) {
-  extern __shared__ uint32_t smem[];
+  extern __shared__ __align__(16) uint32_t smem[];
   ntt_pass_tile<B, false>(p, blockIdx.x, smem);
 }
 
@@ -293,7 +294,7 @@ __device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t* p) {
 __global__ void __launch_bounds__(256, 2) ntt_batch_kernel(const BatchPass* passes, uint32_t npass,
                                                           uint32_t total_tiles, uint32_t* next, uint32_t* done,
                                                           uint32_t* err, uint64_t spin_cycles) {
-  extern __shared__ uint32_t smem[];
+  extern __shared__ __align__(16) uint32_t smem[];
   __shared__ uint32_t s_w, s_k, s_stop;
   for (;;) {
     if (threadIdx.x == 0) {
@@ -359,8 +360,8 @@ __global__ void ntt_tiny_kernel(fe* a, uint32_t log_n, fe w, const fe* pre_lo, c
       uint32_t c0[8], c1[8];
       ld_fe_nc(c0, pre_lo + (i & ((1u << pre_shift) - 1)));
       ld_fe_nc(c1, pre_hi + (i >> pre_shift));
-      mul_r29<P_r>(c0, c0, c1);
-      mul_r29<P_r>(in[i], in[i], c0);
+      mul_rp<P_r>(c0, c0, c1);
+      mul_rp<P_r>(in[i], in[i], c0);
       reduce_once<P_r>(in[i], in[i]);
     }
   }
@@ -377,7 +378,7 @@ __global__ void ntt_tiny_kernel(fe* a, uint32_t log_n, fe w, const fe* pre_lo, c
       mul<P_r>(wik, wik, wk);
     }
     if (has_post) {
-      mul_r29<P_r>(acc, acc, post.w);
+      mul_rp<P_r>(acc, acc, post.w);
       reduce_once<P_r>(acc, acc);
     }
   }
@@ -390,7 +391,7 @@ __global__ void pow_seq_kernel(fe* out, fe base, uint64_t count, uint64_t step) 
   const uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (e >= count) return;
   uint32_t r[8];
-  pow_u64_r29<P_r>(r, base.w, e * step);
+  pow_u64_rp<P_r>(r, base.w, e * step);
   st_fe(out + e, r);
 }
 
@@ -403,7 +404,7 @@ __global__ void twist_table_kernel(fe* out, const fe* lo, const fe* hi, uint32_t
   uint32_t a[8], b[8];
   ld_fe_nc(a, lo + (e & ((1ull << shift) - 1)));
   ld_fe_nc(b, hi + (e >> shift));
-  mul_r29<P_r>(a, a, b);
+  mul_rp<P_r>(a, a, b);
   reduce_once<P_r>(a, a);
   st_fe(out + idx, a);
 }
@@ -419,8 +420,8 @@ __global__ void scale_copy_kernel(fe* dst, const fe* src, uint64_t n, uint64_t d
     uint32_t a[8], b[8];
     ld_fe_nc(a, lo + (i & ((1ull << shift) - 1)));
     ld_fe_nc(b, hi + (i >> shift));
-    mul_r29<P_r>(a, a, b);
-    mul_r29<P_r>(v, v, a);
+    mul_rp<P_r>(a, a, b);
+    mul_rp<P_r>(v, v, a);
     reduce_once<P_r>(v, v);
   }
   st_fe(dst + i * dst_stride, v);
@@ -434,9 +435,9 @@ static fe to_fe(const host::Fr& a) {
   std::memcpy(r.w, a.v, 32);
   return r;
 }
-// R-form (x 2^256) -> R'-form (x 2^261): every constant the kernels multiply
-// data by (roots, twists, coset powers, scales) is kept in R' form for mul_r29.
-static fe to_fe_rp(const host::Fr& a) { return to_fe(host::mul(a, host::from_u64(32))); }
+// R-form (x 2^256) -> R'-form (x 2^260): every constant the kernels multiply
+// data by (roots, twists, coset powers, scales) is kept in R' form for mul_rp.
+static fe to_fe_rp(const host::Fr& a) { return to_fe(host::mul(a, host::from_u64(16))); }
 
 static cudaError_t pow_two_level(fe** lo, fe** hi, uint32_t* shift, const host::Fr& base, int log_count,
                                  cudaStream_t s, bool pooled) {
@@ -467,7 +468,7 @@ __global__ void scale_table_kernel(fe* t, fe scale, uint64_t count) {
   if (i >= count) return;
   uint32_t v[8];
   ld_fe(v, t + i);
-  mul_r29<P_r>(v, v, scale.w);
+  mul_rp<P_r>(v, v, scale.w);
   reduce_once<P_r>(v, v);
   st_fe(t + i, v);
 }
@@ -658,7 +659,7 @@ template <int B>
 static cudaError_t launch_pass(const PassParams& pp, uint64_t ncta, cudaStream_t s) {
   constexpr uint32_t M = 1u << B;
   const uint32_t threads = pp.G * (M / 8);
-  const size_t smem = (size_t)8 * pp.G * M * 4 + (size_t)(M / 2) * 36;
+  const size_t smem = (size_t)8 * pp.G * M * 4 + (size_t)(M / 2) * 40;
   static bool attr_set[64] = {false};
   int dev = 0;
   cudaGetDevice(&dev);
@@ -796,7 +797,7 @@ cudaError_t ntt_run(const NttTables& t, fe* d_a, fe* d_tmp, const NttFuse& f, cu
   return cudaSuccess;
 }
 
-static size_t batch_smem_bytes() { return (size_t)8 * 2048 * 4 + (size_t)1024 * 36; }  // B <= 11
+static size_t batch_smem_bytes() { return (size_t)8 * 2048 * 4 + (size_t)1024 * 40; }  // B <= 11
 
 int ntt_batch_grid(int device) {
   static int cached[64] = {0};
