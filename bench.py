@@ -238,7 +238,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     # autotuner (untimed): NTT plans for the LDE's two sizes, the MSM window
     # for 2^22, and batched-transform plans for 2^10..2^20
     tune = {"ms": 0.0}
-    if not args.no_tune:
+    if args.tune_load:
+        tune["loaded"] = zk.tune_load(args.tune_load, device=dev)
+    elif not args.no_tune:
         tune["ms"] += zk.autotune(zk.TUNE_NTT, LOG_N, LOG_N, device=dev)
         tune["ms"] += zk.autotune(zk.TUNE_NTT, LOG_EXT, LOG_EXT, device=dev)
         tune["ms"] += zk.autotune(zk.TUNE_MSM, 22, 22, device=dev)
@@ -246,6 +248,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     tune["ntt_plans"] = {str(k): zk.get_ntt_plan(k, device=dev) for k in list(range(10, 21)) + [LOG_N, LOG_EXT]}
     tune["msm_window_2p22"] = zk.get_msm_window(22, device=dev)
     tune["ms"] = round(tune["ms"], 1)
+    if args.tune_save:
+        zk.tune_save(args.tune_save, device=dev)
 
     def step():
         zk.lagrange_to_extended_dev(d_vals, d_ext, LOG_N, LOG_EXT, c["omega_inv"], c["divisor"], c["g"],
@@ -350,7 +354,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         per_launch_bytes = d["bytes"] / d["launches"]
         roof = {"bound": "imad", "kernel": name, "achieved": round(achieved_imad / 1e12, 3),
                 "peak": round(imad_ps / 1e12, 3), "unit": "TIMAD/s",
-                "frac": round(achieved_imad / imad_ps, 4), "traffic": TRAFFIC.get(name),
+                "frac": round(achieved_imad / imad_ps, 4), "traffic": (round(TRAFFIC_RATIO[name] * per_launch_bytes) if name in TRAFFIC_RATIO else None),
+                "traffic_source": TRAFFIC_SOURCE.get(name),
                 "algorithmic_bytes_per_launch": per_launch_bytes,
                 "hbm_gbs": round(d["bytes"] / (d["ms"] * 1e-3) / 1e9, 1),
                 "hbm_frac_of_measured": round(d["bytes"] / (d["ms"] * 1e-3) / 1e9 / HBM_GBS, 4),
@@ -605,6 +610,15 @@ def bench_serving(zk, torch, dev: int, njobs: int = 1000, rate: float = 2000.0, 
     lat_pc, span_pc = run_plain(False)
     srv.close()
     n = len(trace)
+    # host<->device bytes the trace moves, against the pinned-copy bandwidth
+    # of this box measured the same way (1 GiB, CUDA events)
+    h2d = sum((1 << k) * 32 for _, kind, k in trace)
+    d2h = sum(96 if kind == "msm" else (1 << (k + 2 if kind == "lde" else k)) * 32 for _, kind, k in trace)
+    pcie = pcie_bandwidth(torch, dev)
+    pcie.update({"trace_h2d_gb": round(h2d / 1e9, 2), "trace_d2h_gb": round(d2h / 1e9, 2),
+                 "batched_closed_loop_d2h_gbs": round(d2h / span_sc / 1e9, 2),
+                 "batched_closed_loop_h2d_gbs": round(h2d / span_sc / 1e9, 2),
+                 "one_call_closed_loop_d2h_gbs": round(d2h / span_pc / 1e9, 2)})
     return {
         "jobs": n, "offered_rate_jobs_s": rate, "mix": "35% NTT 2^12-2^22, 35% coset LDE x4 2^12-2^22, "
                                                          "30% MSM 2^14-2^20 (resident bases)",
@@ -619,7 +633,45 @@ def bench_serving(zk, torch, dev: int, njobs: int = 1000, rate: float = 2000.0, 
             "batched_p99_ms": round(pct(lat_sc, 99) * 1e3, 3), "one_call_p99_ms": round(pct(lat_pc, 99) * 1e3, 3)},
         "server": {"waves": st["waves"], "batch_launches": st["batch_launches"], "hbm_peak_gb":
                    round(st["hbm_peak"] / 1e9, 2), "rejected": st["rejected"], "failed": st["failed"]},
+        "pcie": pcie,
     }
+
+
+def pcie_bandwidth(torch, dev: int, nbytes: int = 1 << 30) -> dict:
+    """Pinned host<->device copy bandwidth: H2D alone, D2H alone, and both at
+    once on two streams (GB/s, best of 3, CUDA events)."""
+    h_in = torch.empty(nbytes // 8, dtype=torch.int64).pin_memory()
+    h_out = torch.empty(nbytes // 8, dtype=torch.int64).pin_memory()
+    d_a = torch.empty(nbytes // 8, dtype=torch.int64, device=f"cuda:{dev}")
+    d_b = torch.zeros(nbytes // 8, dtype=torch.int64, device=f"cuda:{dev}")
+    s1, s2 = torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev)
+
+    def timed(fn) -> float:
+        best = 1e30
+        for _ in range(3):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            fn()
+            torch.cuda.synchronize()
+            best = min(best, time.perf_counter() - t0)
+        return best
+
+    def h2d():
+        with torch.cuda.stream(s1):
+            d_a.copy_(h_in, non_blocking=True)
+
+    def d2h():
+        with torch.cuda.stream(s2):
+            h_out.copy_(d_b, non_blocking=True)
+
+    def both():
+        h2d()
+        d2h()
+
+    t_h, t_d, t_b = timed(h2d), timed(d2h), timed(both)
+    del d_a, d_b
+    return {"pinned_h2d_gbs": round(nbytes / t_h / 1e9, 1), "pinned_d2h_gbs": round(nbytes / t_d / 1e9, 1),
+            "pinned_duplex_gbs": round(2 * nbytes / t_b / 1e9, 1)}
 
 
 def small_fr(n: int, seed: int, bits: int = 16) -> np.ndarray:
@@ -649,7 +701,13 @@ def msm_roofline(prof: dict, imad_ps: float, n: int, total_ms: float):
 
 
 HBM_GBS = 6543.1
-TRAFFIC: dict = {}
+# DRAM bytes (read + write) per launch over algorithmic bytes, from one ncu
+# capture of the same kernel on a smaller case (traffic grows with the
+# elements processed): ntt_pass_kernel<6> on a 2^24 transform, plan 6+6+6+6,
+# launches 1.583 / 1.611 GB and 1.034 / 1.082 GB.
+TRAFFIC_RATIO = {"ntt_pass_b6": 0.97}
+TRAFFIC_SOURCE = {"ntt_pass_b6": "ncu dram__bytes_read.sum + dram__bytes_write.sum of ntt_pass_kernel<6> on a "
+                                 "2^24 transform (plan 6+6+6+6), scaled by algorithmic bytes"}
 
 
 def _load_peaks():
@@ -673,6 +731,8 @@ def run_case(args):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if args.case in ("ntt22", "lde20", "ntt24"):
         k = {"ntt22": 22, "lde20": 20, "ntt24": 24}[args.case]
+        if args.plan:  # pass widths for the transform of this case (the extended one for lde20)
+            zk.set_ntt_plan(k + 2 if args.case == "lde20" else k, [int(b) for b in args.plan.split(",")])
         c = lde_constants(k, 2)
         d = torch.from_numpy(rand_fr(1 << k, 7).view(np.int64)).cuda()
         ext = torch.empty(((1 << (k + 2)), 4), dtype=torch.int64, device="cuda") if args.case == "lde20" else None
@@ -724,6 +784,9 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="use the built-in NTT plans and MSM windows")
     ap.add_argument("--case", choices=["ntt22", "ntt24", "lde20", "msm20"], default=None,
                     help="run a small profiling case instead of the benchmark")
+    ap.add_argument("--plan", default=None, help="with --case: NTT pass widths, e.g. 6,6,6,6")
+    ap.add_argument("--tune-save", default=None, help="write the autotuner's choices to this file")
+    ap.add_argument("--tune-load", default=None, help="load autotuner choices from this file instead of tuning")
     args = ap.parse_args()
     _load_peaks()
     rank = int(os.environ.get("RANK", 0))
