@@ -241,11 +241,14 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     if args.tune_load:
         tune["loaded"] = zk.tune_load(args.tune_load, device=dev)
     elif not args.no_tune:
-        tune["ms"] += zk.autotune(zk.TUNE_NTT, LOG_N, LOG_N, device=dev)
+        # single transforms 2^21..2^24 (the LDE's 2^24, the serving mix's large
+        # NTT / LDE sizes) and 2^26; MSM windows for every size the bench runs
+        tune["ms"] += zk.autotune(zk.TUNE_NTT, 21, LOG_N, device=dev)
         tune["ms"] += zk.autotune(zk.TUNE_NTT, LOG_EXT, LOG_EXT, device=dev)
-        tune["ms"] += zk.autotune(zk.TUNE_MSM, 22, 22, device=dev)
+        tune["ms"] += zk.autotune(zk.TUNE_MSM, 14, 22, device=dev)
         tune["ms"] += zk.autotune(zk.TUNE_NTT_BATCHED, 10, 20, device=dev)
-    tune["ntt_plans"] = {str(k): zk.get_ntt_plan(k, device=dev) for k in list(range(10, 21)) + [LOG_N, LOG_EXT]}
+    tune["ntt_plans"] = {str(k): zk.get_ntt_plan(k, device=dev) for k in list(range(10, 25)) + [LOG_EXT]}
+    tune["msm_windows"] = {str(k): zk.get_msm_window(k, device=dev) for k in range(14, 23)}
     tune["msm_window_2p22"] = zk.get_msm_window(22, device=dev)
     tune["ms"] = round(tune["ms"], 1)
     if args.tune_save:
@@ -609,6 +612,33 @@ def bench_serving(zk, torch, dev: int, njobs: int = 1000, rate: float = 2000.0, 
     lat_p, span_p = run_plain(True)
     lat_pc, span_pc = run_plain(False)
     srv.close()
+
+    # device time of each job alone (inputs resident, no copies; best of 3),
+    # summed over the trace: the compute floor of any schedule on one GPU
+    dev_ms = {}
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for kind, k in pools:
+        ti, a, to, o = pools[(kind, k)]
+        d = ti.to(f"cuda:{dev}")
+        e = torch.empty((1 << (k + 2), 4), dtype=torch.int64, device=f"cuda:{dev}") if kind == "lde" else None
+        best = 1e30
+        for _ in range(4):
+            ev0.record(stream)
+            if kind == "ntt":
+                zk.ntt_dev(d, k, consts[k]["omega"], stream=stream)
+            elif kind == "lde":
+                zk.lagrange_to_extended_dev(d, e, k, k + 2, consts[k]["omega_inv"], consts[k]["divisor"], g7,
+                                            consts[k + 2]["omega"], stream=stream)
+            else:
+                zk.msm_dev(d, d_bases[: 1 << k], d_out, stream=stream)
+            ev1.record(stream)
+            stream.synchronize()
+            best = min(best, ev0.elapsed_time(ev1))
+        dev_ms[(kind, k)] = best
+        del d, e
+    trace_dev_s = sum(dev_ms[(kind, k)] for _, kind, k in trace) / 1e3
+    by_kind = {kd: round(sum(dev_ms[(kind, k)] for _, kind, k in trace if kind == kd) / 1e3, 3)
+               for kd in ("ntt", "lde", "msm")}
     n = len(trace)
     # host<->device bytes the trace moves, against the pinned-copy bandwidth
     # of this box measured the same way (1 GiB, CUDA events)
@@ -634,6 +664,9 @@ def bench_serving(zk, torch, dev: int, njobs: int = 1000, rate: float = 2000.0, 
         "server": {"waves": st["waves"], "batch_launches": st["batch_launches"], "hbm_peak_gb":
                    round(st["hbm_peak"] / 1e9, 2), "rejected": st["rejected"], "failed": st["failed"]},
         "pcie": pcie,
+        "device_floor": {"trace_device_s": round(trace_dev_s, 3), "by_kind_s": by_kind,
+                         "jobs_s_at_floor": round(n / trace_dev_s, 1),
+                         "batched_closed_loop_frac_of_floor": round(trace_dev_s / span_sc, 3)},
     }
 
 

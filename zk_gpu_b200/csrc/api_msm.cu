@@ -19,23 +19,29 @@ int msm_host(int device, const uint64_t* scalars, const uint64_t* bases_xy, uint
   cudaStream_t s;
   int st = zk::bind_device(device, &s);
   if (st) return st;
-  fe *ds = nullptr, *db = nullptr, *dout = nullptr;
+  // the per-window sums come back to the host, which does the Horner step
+  // (host::fq::msm_combine_windows) and the normalisation
+  fe *ds = nullptr, *db = nullptr, *dwin = nullptr;
+  uint64_t win[zk::MSM_MAX_WINDOWS * 16];
   cudaError_t e = cudaMallocAsync((void**)&ds, n * 32, s);
   if (e == cudaSuccess) e = cudaMallocAsync((void**)&db, n * 64, s);
-  if (e == cudaSuccess) e = cudaMallocAsync((void**)&dout, 96, s);
+  if (e == cudaSuccess) e = cudaMallocAsync((void**)&dwin, zk::MSM_MAX_WINDOWS * 128, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(ds, scalars, n * 32, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(db, bases_xy, n * 64, cudaMemcpyHostToDevice, s);
   uint64_t nl = 0;
-  if (e == cudaSuccess) e = zk::msm_run(ds, db, n, dout, s, 0, &nl);
+  zk::MsmWindowsOut wo;
+  wo.d_winsum = dwin;
+  if (e == cudaSuccess) e = zk::msm_run(ds, db, n, nullptr, s, 0, &nl, &wo);
   zk::count_launches(nl);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(out, dout, 96, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess && wo.windows > zk::MSM_MAX_WINDOWS) e = cudaErrorInvalidValue;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(win, dwin, wo.windows * 128ull, cudaMemcpyDeviceToHost, s);
   if (ds) cudaFreeAsync(ds, s);
   if (db) cudaFreeAsync(db, s);
-  if (dout) cudaFreeAsync(dout, s);
+  if (dwin) cudaFreeAsync(dwin, s);
   cudaError_t e2 = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return zk::status_of("msm", e);
   if (e2 != cudaSuccess) return zk::status_of("msm sync", e2);
-  zk::host::fq::normalize_jacobian(out);
+  zk::host::fq::msm_combine_windows(win, wo.windows, wo.c, out);
   return ZKGPU_OK;
 }
 

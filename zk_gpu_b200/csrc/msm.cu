@@ -310,14 +310,24 @@ __global__ void zero_out_kernel(fe* out) {
 }
 
 cudaError_t msm_run(const fe* d_scalars, const fe* d_bases, uint64_t n, fe* d_out, cudaStream_t s, int c_override,
-                    uint64_t* launches) {
+                    uint64_t* launches, MsmWindowsOut* wout) {
   uint64_t nl = 0;
   if (n == 0) {
+    if (wout) {
+      wout->windows = 0;
+      if (launches) *launches = 0;
+      return cudaSuccess;
+    }
     zero_out_kernel<<<1, 32, 0, s>>>(d_out);
     if (launches) *launches = 1;
     return cudaGetLastError();
   }
   const MsmPlan p = make_msm_plan(n, c_override);
+  if (wout) {
+    if ((uint32_t)p.windows > MSM_MAX_WINDOWS || !wout->d_winsum) return cudaErrorInvalidValue;
+    wout->windows = (uint32_t)p.windows;
+    wout->c = (uint32_t)p.c;
+  }
   const uint32_t W = (uint32_t)p.windows, B = p.buckets, L = p.seg_len;
   const uint32_t total = W * B;
   const uint32_t nblk = (total + 1023) / 1024;
@@ -347,7 +357,10 @@ cudaError_t msm_run(const fe* d_scalars, const fe* d_bases, uint64_t n, fe* d_ou
   alloc((void**)&subres, max_sub * 128ull);
   alloc((void**)&buckets, total * 128ull);
   alloc((void**)&segres, segs * 128ull);
-  alloc((void**)&winsum, W * 128ull);
+  if (wout)
+    winsum = wout->d_winsum;  // caller's buffer, left for the host's Horner step
+  else
+    alloc((void**)&winsum, W * 128ull);
   alloc((void**)&bases_rp, n * 64ull);
   if (e == cudaSuccess) {
     const double nd = (double)n;
@@ -388,13 +401,13 @@ cudaError_t msm_run(const fe* d_scalars, const fe* d_bases, uint64_t n, fe* d_ou
       msm_segment_kernel<<<(segs + 127) / 128, 128, 0, s>>>(buckets, segres, B, L, segs);
     }
     msm_window_kernel<<<W, 256, 0, s>>>(segres, winsum, B / L);
-    msm_combine_kernel<<<1, 32, 0, s>>>(winsum, W, (uint32_t)p.c, d_out);
-    nl = 17;
+    if (!wout) msm_combine_kernel<<<1, 32, 0, s>>>(winsum, W, (uint32_t)p.c, d_out);
+    nl = wout ? 16 : 17;
     e = cudaGetLastError();
   }
   for (void* ptr : {(void*)counts, (void*)offsets, (void*)cursor, (void*)bsums, (void*)list, (void*)nsub,
                     (void*)sub_off, (void*)sub2b, (void*)heavy, (void*)heavy_count, (void*)subres, (void*)buckets,
-                    (void*)segres, (void*)winsum, (void*)bases_rp})
+                    (void*)segres, (void*)(wout ? nullptr : winsum), (void*)bases_rp})
     if (ptr) cudaFreeAsync(ptr, s);
   if (launches) *launches = nl;
   return e;

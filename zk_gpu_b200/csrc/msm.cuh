@@ -36,7 +36,16 @@ int tuned_msm_window(int device, int log_n);
 
 // Enqueue the MSM on `s`; d_out receives the Jacobian sum (X, Y, Z: 12 u64,
 // not normalised; identity = Z 0).  Scratch comes from the stream pool.
+// Optional: stop before the last step and leave the per-window sums for the
+// host (host::fq::msm_combine_windows), which does the ~250 dependent
+// doublings of the Horner step far faster than one GPU thread.
+struct MsmWindowsOut {
+  fe* d_winsum = nullptr;  // >= plan.windows * 4 elements (XYZZ, R' form)
+  uint32_t windows = 0;    // set by msm_run (0 for n = 0)
+  uint32_t c = 0;
+};
+constexpr uint32_t MSM_MAX_WINDOWS = 64;  // c >= 4
 cudaError_t msm_run(const fe* d_scalars, const fe* d_bases_xy, uint64_t n, fe* d_out, cudaStream_t s,
-                    int c_override = 0, uint64_t* launches = nullptr);
+                    int c_override = 0, uint64_t* launches = nullptr, MsmWindowsOut* wout = nullptr);
 
 }  // namespace zk

@@ -60,7 +60,7 @@ struct Wave {
   cudaStream_t s_ntt = nullptr, s_msm = nullptr;
   cudaEvent_t ev_ntt = nullptr, ev_msm = nullptr;
   std::vector<BatchPass> passes;  // host copy kept alive for the async upload
-  uint64_t* mailbox = nullptr;    // pinned: [0] batch error flag, then 12 words per MSM job
+  uint64_t* mailbox = nullptr;    // pinned: [0] batch error flag, then kMsmSlotWords per MSM job
   int status = ZKGPU_OK;
 };
 
@@ -84,7 +84,7 @@ class Server {
     grid_ = ntt_batch_grid(device_);
     // one pinned mailbox per stream slot; a slot is reused only after the
     // wave that used it retired (waves retire in launch order)
-    slot_words_ = 2 + 12 * (uint64_t)max_wave_;
+    slot_words_ = 2 + kMsmSlotWords * (uint64_t)max_wave_;
     ZK_TRY("cudaMallocHost(mailbox)", cudaMallocHost((void**)&mailbox_, kStreams * slot_words_ * 8));
     sched_ = std::thread([this] { sched_loop(); });
     comp_ = std::thread([this] { comp_loop(); });
@@ -184,6 +184,9 @@ class Server {
 
  private:
   static constexpr int kStreams = 4;
+  static constexpr int kEagerWaves = 2;
+  // per MSM job in a wave's mailbox: window count, c, then the window sums
+  static constexpr uint64_t kMsmSlotWords = 2 + 16 * (uint64_t)MSM_MAX_WINDOWS;
 
   void sched_loop() {
     cudaSetDevice(device_);
@@ -192,7 +195,15 @@ class Server {
       std::vector<JobRec*> batch;
       {
         std::unique_lock<std::mutex> lk(mu_);
-        cv_sched_.wait(lk, [&] { return stop_ || (adm_.pending() > 0 && waves_inflight_ < kStreams); });
+        // Continuous batching: with fewer than kEagerWaves waves on the GPU a
+        // wave starts with whatever is pending (low latency at low load);
+        // with more in flight the GPU has queued work, so the next wave waits
+        // until a full wave is pending or a wave retires (bigger waves, fewer
+        // launches and better overlap under load).
+        cv_sched_.wait(lk, [&] {
+          return stop_ || (adm_.pending() > 0 && waves_inflight_ < kStreams &&
+                           (waves_inflight_ < kEagerWaves || adm_.pending() >= max_wave_));
+        });
         if (stop_) return;
         const uint64_t gen = retired_gen_;
         for (uint64_t t : adm_.admit(max_wave_)) batch.push_back(jobs_.at(t).get());
@@ -250,19 +261,26 @@ class Server {
     for (JobRec* r : w.jobs) {
       const zkgpu_job& j = r->job;
       if (j.kind == ZKGPU_KIND_MSM) {
-        fe *ds = nullptr, *dout = nullptr;
+        // the window sums come back to the mailbox; the completion thread
+        // does the Horner step on the host (host::fq::msm_combine_windows)
+        fe *ds = nullptr, *dwin = nullptr;
         const BaseSet& bs = bases_[j.bases_id];
         if (ok(cudaMallocAsync((void**)&ds, std::max<uint64_t>(j.n, 1) * 32, w.s_msm)) &&
-            ok(cudaMallocAsync((void**)&dout, 96, w.s_msm)) &&
+            ok(cudaMallocAsync((void**)&dwin, MSM_MAX_WINDOWS * 128, w.s_msm)) &&
             ok(cudaMemcpyAsync(ds, j.input, j.n * 32, cudaMemcpyHostToDevice, w.s_msm))) {
           uint64_t nl = 0;
-          ok(msm_run(ds, bs.d, j.n, dout, w.s_msm, 0, &nl));
-          r->msm_out = next_msm_slot;
-          next_msm_slot += 12;
-          ok(cudaMemcpyAsync(r->msm_out, dout, 96, cudaMemcpyDeviceToHost, w.s_msm));
+          MsmWindowsOut wo;
+          wo.d_winsum = dwin;
+          if (ok(msm_run(ds, bs.d, j.n, nullptr, w.s_msm, 0, &nl, &wo))) {
+            r->msm_out = next_msm_slot;
+            next_msm_slot += kMsmSlotWords;
+            r->msm_out[0] = wo.windows;
+            r->msm_out[1] = wo.c;
+            ok(cudaMemcpyAsync(r->msm_out + 2, dwin, wo.windows * 128ull, cudaMemcpyDeviceToHost, w.s_msm));
+          }
         }
         frees_msm.push_back(ds);
-        frees_msm.push_back(dout);
+        frees_msm.push_back(dwin);
         continue;
       }
       const bool lde = j.kind == ZKGPU_KIND_LDE;
@@ -401,8 +419,9 @@ class Server {
       const auto now = clk::now();
       for (JobRec* r : w->jobs)
         if (st == ZKGPU_OK && r->job.kind == ZKGPU_KIND_MSM && r->msm_out) {
-          host::fq::normalize_jacobian(r->msm_out);
-          std::memcpy(r->job.output, r->msm_out, 96);
+          uint64_t out[12];
+          host::fq::msm_combine_windows(r->msm_out + 2, (uint32_t)r->msm_out[0], (uint32_t)r->msm_out[1], out);
+          std::memcpy(r->job.output, out, 96);
         }
       cudaEventDestroy(w->ev_ntt);
       cudaEventDestroy(w->ev_msm);
