@@ -22,7 +22,13 @@ MsmPlan make_msm_plan(uint64_t n, int c_override) {
   p.c = c;
   p.windows = (254 + c - 1) / c;
   p.buckets = 1u << (c - 1);
-  p.seg_len = std::min<uint32_t>(16u, p.buckets);
+  // buckets per reduction segment: each segment thread's latency is its
+  // running sum (2L additions) plus the weight multiply lo * S (about c
+  // doublings).  Few buckets per window: short segments (L = 4) for
+  // parallelism; many (2^12 and up): L = 16, since the extra weight
+  // multiplies of 4x more segments cost more than they save (measured on
+  // B200: 2^14 points, c = 10: 0.57 -> 0.24 ms; 2^22, c = 15: 0.9 -> 1.6 ms)
+  p.seg_len = std::min<uint32_t>(p.buckets >= 4096 ? 16u : 4u, p.buckets);
   return p;
 }
 
@@ -129,12 +135,13 @@ __global__ void scan_add_kernel(uint32_t* out, uint32_t* cursor, const uint32_t*
 // each, so a bucket that collects a large share of the points (skewed
 // scalars, e.g. many small ones all carrying into the same digit) is summed
 // by many threads instead of one.
-constexpr uint32_t SUB = 64;          // entries per sub-bucket
+constexpr uint32_t SUB_MAX = 64;      // entries per sub-bucket (large MSMs)
+constexpr uint32_t SUB_MIN = 16;      // small MSMs: shorter chains, more threads
 constexpr uint32_t SEQ_MAX = 16;      // sub-sums a bucket combines in one thread
 
-__global__ void msm_nsub_kernel(const uint32_t* counts, uint32_t* nsub, uint32_t total) {
+__global__ void msm_nsub_kernel(const uint32_t* counts, uint32_t* nsub, uint32_t total, uint32_t sub_len) {
   const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b < total) nsub[b] = (counts[b] + SUB - 1) / SUB;
+  if (b < total) nsub[b] = (counts[b] + sub_len - 1) / sub_len;
 }
 
 __global__ void msm_submap_kernel(const uint32_t* nsub, const uint32_t* sub_off, uint32_t* sub2b, uint32_t total) {
@@ -148,13 +155,13 @@ __global__ void msm_submap_kernel(const uint32_t* nsub, const uint32_t* sub_off,
 __global__ void __launch_bounds__(256) msm_subbucket_kernel(const uint32_t* list, const uint32_t* offsets,
                                                             const uint32_t* counts, const uint32_t* sub_off,
                                                             const uint32_t* sub2b, const uint32_t* total_sub,
-                                                            const fe* bases, fe* subres) {
+                                                            const fe* bases, fe* subres, uint32_t sub_len) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= *total_sub) return;
   const uint32_t b = sub2b[s];
   const uint32_t j = s - sub_off[b];
-  const uint32_t beg = offsets[b] + j * SUB;
-  const uint32_t end = min(offsets[b] + counts[b], beg + SUB);
+  const uint32_t beg = offsets[b] + j * sub_len;
+  const uint32_t end = min(offsets[b] + counts[b], beg + sub_len);
   xyzz_t acc;
   xyzz_set_inf(acc);
   for (uint32_t k = beg; k < end; k++) {
@@ -337,9 +344,12 @@ cudaError_t msm_run(const fe* d_scalars, const fe* d_bases, uint64_t n, fe* d_ou
   uint32_t *nsub = nullptr, *sub_off = nullptr, *sub2b = nullptr, *heavy = nullptr, *heavy_count = nullptr;
   fe *buckets = nullptr, *segres = nullptr, *winsum = nullptr, *subres = nullptr, *bases_rp = nullptr;
   const uint32_t segs = total / L;
-  // sum_b ceil(count_b / SUB) <= entries / SUB + total; heavy buckets have > SEQ_MAX * SUB entries
-  const uint64_t max_sub = entries / SUB + total + 1;
-  const uint64_t max_heavy = entries / ((uint64_t)SEQ_MAX * SUB) + 1;
+  // sub-bucket size: enough sub-buckets to fill the GPU (about 2^17 threads)
+  uint32_t sub_len = SUB_MAX;
+  while (sub_len > SUB_MIN && entries / sub_len < (1ull << 17)) sub_len >>= 1;
+  // sum_b ceil(count_b / sub_len) <= entries / sub_len + total; heavy buckets have > SEQ_MAX * sub_len entries
+  const uint64_t max_sub = entries / sub_len + total + 1;
+  const uint64_t max_heavy = entries / ((uint64_t)SEQ_MAX * sub_len) + 1;
   cudaError_t e = cudaSuccess;
   auto alloc = [&](void** ptr, size_t bytes) {
     if (e == cudaSuccess) e = cudaMallocAsync(ptr, bytes, s);
@@ -380,7 +390,7 @@ cudaError_t msm_run(const fe* d_scalars, const fe* d_bases, uint64_t n, fe* d_ou
       ProfScope ps("msm_scatter", s, nd, nd * 32 + (double)entries * 4);
       msm_scatter_kernel<<<g, 256, 0, s>>>(d_scalars, n, (uint32_t)p.c, W, cursor, list);
     }
-    msm_nsub_kernel<<<gb, 256, 0, s>>>(counts, nsub, total);
+    msm_nsub_kernel<<<gb, 256, 0, s>>>(counts, nsub, total, sub_len);
     scan_block_kernel<<<nblk, 1024, 0, s>>>(nsub, sub_off, bsums, total);
     scan_sums_kernel<<<1, 1024, 0, s>>>(bsums, nblk, sub_off + total);
     scan_add_kernel<<<nblk, 1024, 0, s>>>(sub_off, cursor, bsums, total);
@@ -389,7 +399,7 @@ cudaError_t msm_run(const fe* d_scalars, const fe* d_bases, uint64_t n, fe* d_ou
       // convention: 6 Fq products per point-window (batch-affine cost)
       ProfScope ps("msm_bucket", s, (double)entries * 6, (double)entries * (64 + 4) + max_sub * 128.0);
       msm_subbucket_kernel<<<(unsigned)((max_sub + 255) / 256), 256, 0, s>>>(list, offsets, counts, sub_off, sub2b,
-                                                                              sub_off + total, bases_rp, subres);
+                                                                              sub_off + total, bases_rp, subres, sub_len);
     }
     {
       ProfScope ps("msm_bucket_final", s, (double)total * 14, total * 256.0);

@@ -36,7 +36,7 @@ uint64_t msm_scratch_bytes(uint64_t n) {
   const MsmPlan p = make_msm_plan(n);
   const uint64_t total = (uint64_t)p.windows * p.buckets;
   const uint64_t entries = n * p.windows;
-  const uint64_t max_sub = entries / 64 + total + 1;
+  const uint64_t max_sub = entries / 16 + total + 1;  // smallest sub-bucket size msm_run uses
   return total * 4 * 6 + entries * 4 + max_sub * (4 + 128) + total * 128 * 2 + 4096;
 }
 
