@@ -87,7 +87,7 @@ uint64_t parallel_msm_api(size_t device_id, const uint64_t *data, const GpuAffin
                           GpuProjective *acc);
 
 /* ======================================================================
- * Host-buffer API with the north-star names (fft / ifft / coset_fft / msm).
+ * Host-buffer API with short names (fft / ifft / coset_fft / msm).
  * ====================================================================== */
 int zkgpu_fft(int device, uint64_t *a, uint32_t log_n, const uint64_t omega[4]);
 int zkgpu_ifft(int device, uint64_t *a, uint32_t log_n, const uint64_t omega_inv[4], const uint64_t divisor[4]);

@@ -159,7 +159,7 @@ def test_invalid_omega_rejected(zk, oracle):
 
 
 def test_full_size_fft_2p24(zk, oracle):
-    """north-star size, bit-exact against the oracle"""
+    """the 2^24 transform, bit-exact against the oracle"""
     log_n = 24
     a = oracle.rand_fr(1 << log_n, 24)
     w = oracle.omega(log_n)

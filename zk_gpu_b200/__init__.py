@@ -175,7 +175,7 @@ def parallel_msm_api(device_id: int, data: np.ndarray, bases: np.ndarray, length
 
 
 # ---------------------------------------------------------------------------
-# north-star names: fft / ifft / coset_fft / msm (return new arrays, raise)
+# short names: fft / ifft / coset_fft / msm (return new arrays, raise)
 # ---------------------------------------------------------------------------
 def fft(a: np.ndarray, omega, log_n: int, device: int = 0) -> np.ndarray:
     out = np.array(_arr(a), copy=True)

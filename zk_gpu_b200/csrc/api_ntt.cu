@@ -200,7 +200,7 @@ extern "C" uint64_t parallel_coeff_to_extended_part_api(size_t device_id, uint64
 }
 
 // ===========================================================================
-// north-star names, host buffers
+// short names (fft / ifft / coset_fft / msm), host buffers
 // ===========================================================================
 extern "C" int zkgpu_fft(int device, uint64_t* a, uint32_t log_n, const uint64_t omega[4]) {
   return ntt_host(device, a, log_n, omega, nullptr, nullptr);
