@@ -132,3 +132,22 @@ def test_g1_mul_fixed_matches_oracle_bases(zk, oracle):
     assert np.array_equal(got[2][:4], zk.G1_GENERATOR[:4])
     assert np.array_equal(got[2][4:], oracle.to_mont(q - 2, oracle.FQ))
     assert np.array_equal(got[3:], pts[3:])
+
+
+@pytest.mark.parametrize("n", [1, 300, 1 << 14, 1 << 17])
+def test_msm_host_and_device_horner_agree(zk, oracle, n):
+    """the host-buffer call finishes the windows' Horner step on the host, the
+    device call on the GPU: both must give the same (normalised) point"""
+    import torch
+    s = oracle.rand_fr(n, 700 + n)
+    pts = oracle.rand_bases(n, 701 + n)
+    host = zk.msm(s, pts)
+    d_s = torch.from_numpy(s.view(np.int64)).cuda()
+    d_b = torch.from_numpy(pts.view(np.int64)).cuda()
+    d_o = torch.zeros(12, dtype=torch.int64, device="cuda")
+    zk.msm_dev(d_s, d_b, d_o)
+    torch.cuda.synchronize()
+    jac = d_o.cpu().numpy().view(np.uint64)
+    assert np.array_equal(affine_of(host), oracle.g1_normalize(jac))
+    if n <= 1 << 14:
+        assert np.array_equal(affine_of(host), oracle.multiexp(s, pts))

@@ -111,3 +111,27 @@ def test_server_concurrent_submitters(zk, oracle):
         t.join()
     assert not errors
     srv.close()
+
+
+def test_server_msm_edge_sizes(zk, oracle):
+    """MSM jobs of 0, 1, 2, 257 and 5000 points in one wave: the window sums
+    come back to the host, whose Horner step must give the oracle's point"""
+    srv = zk.Server(device=0, hbm_budget=8 * 10**9, max_wave_jobs=8)
+    bases, k = oracle.rand_bases(5000, 15, with_dlog=True)
+    bid = srv.add_bases(bases)
+    jobs = []
+    for i, n in enumerate([0, 1, 2, 257, 5000]):
+        s = oracle.rand_fr(max(n, 1), 600 + i)[:n]
+        out = np.full(12, 7, np.uint64)
+        jobs.append((zk.msm_job(s, out, n, bid), s, out, n))
+    tickets = [srv.submit(j[0]) for j in jobs]
+    for t in tickets:
+        srv.wait(t, timeout_ms=60000)
+    for jb, s, out, n in jobs:
+        if n == 0:
+            assert not out.any()
+            continue
+        ref = oracle.msm_by_dlog(s, k[:n])
+        assert np.array_equal(out[:8], ref)
+        assert np.array_equal(out[8:], oracle.to_mont(1, oracle.FQ))
+    srv.close()
