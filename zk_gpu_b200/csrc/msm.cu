@@ -63,25 +63,45 @@ __device__ __forceinline__ void for_each_digit(const fe* scalar, uint32_t c, uin
   }
 }
 
-__global__ void msm_count_kernel(const fe* scalars, uint64_t n, uint32_t c, uint32_t windows, uint32_t* counts) {
+// Several MSMs over one base array in one pass: scalars of job j occupy
+// [off[j], off[j+1]) of the concatenated scalar array, its windows are
+// j * windows + w, and its entries name the base by the local index.
+__device__ __forceinline__ uint32_t job_of(const uint32_t* off, uint32_t jobs, uint32_t i) {
+  uint32_t lo = 0, hi = jobs;  // off[lo] <= i < off[hi]
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (off[mid] <= i) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void msm_count_kernel(const fe* scalars, uint64_t n, uint32_t c, uint32_t windows, uint32_t* counts,
+                                 const uint32_t* job_off, uint32_t jobs) {
   const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint32_t B = 1u << (c - 1);
+  const uint32_t w0 = jobs > 1 ? job_of(job_off, jobs, (uint32_t)i) * windows : 0u;
   for_each_digit(scalars + i, c, windows, [&](uint32_t w, int d) {
     const uint32_t mag = (uint32_t)(d < 0 ? -d : d);
-    atomicAdd(&counts[w * B + mag - 1], 1u);
+    atomicAdd(&counts[(w0 + w) * B + mag - 1], 1u);
   });
 }
 
 __global__ void msm_scatter_kernel(const fe* scalars, uint64_t n, uint32_t c, uint32_t windows, uint32_t* cursor,
-                                   uint32_t* list) {
+                                   uint32_t* list, const uint32_t* job_off, uint32_t jobs) {
   const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint32_t B = 1u << (c - 1);
+  uint32_t w0 = 0, local = (uint32_t)i;
+  if (jobs > 1) {
+    const uint32_t j = job_of(job_off, jobs, (uint32_t)i);
+    w0 = j * windows;
+    local = (uint32_t)i - job_off[j];
+  }
   for_each_digit(scalars + i, c, windows, [&](uint32_t w, int d) {
     const uint32_t mag = (uint32_t)(d < 0 ? -d : d);
-    const uint32_t pos = atomicAdd(&cursor[w * B + mag - 1], 1u);
-    list[pos] = (uint32_t)i | (d < 0 ? 0x80000000u : 0u);
+    const uint32_t pos = atomicAdd(&cursor[(w0 + w) * B + mag - 1], 1u);
+    list[pos] = local | (d < 0 ? 0x80000000u : 0u);
   });
 }
 
@@ -316,8 +336,13 @@ __global__ void zero_out_kernel(fe* out) {
   }
 }
 
-cudaError_t msm_run(const fe* d_scalars, const fe* d_bases, uint64_t n, fe* d_out, cudaStream_t s, int c_override,
-                    uint64_t* launches, MsmWindowsOut* wout) {
+namespace {
+// n: scalars (all jobs); jobs > 1: job_off (device, jobs + 1 entries) splits
+// them and every job reads bases [0, nbases); the window sums of job j are
+// windows [j W, (j + 1) W) of wout.
+cudaError_t msm_run_impl(const fe* d_scalars, const fe* d_bases, uint64_t n, fe* d_out, cudaStream_t s,
+                         int c_override, uint64_t* launches, MsmWindowsOut* wout, const uint32_t* job_off,
+                         uint32_t jobs, uint64_t nbases) {
   uint64_t nl = 0;
   if (n == 0) {
     if (wout) {
@@ -329,16 +354,20 @@ cudaError_t msm_run(const fe* d_scalars, const fe* d_bases, uint64_t n, fe* d_ou
     if (launches) *launches = 1;
     return cudaGetLastError();
   }
-  const MsmPlan p = make_msm_plan(n, c_override);
+  if (jobs == 0) jobs = 1;
+  // one window size for every job: the plan of the mean job size
+  const MsmPlan p = make_msm_plan((n + jobs - 1) / jobs, c_override);
   if (wout) {
     if ((uint32_t)p.windows > MSM_MAX_WINDOWS || !wout->d_winsum) return cudaErrorInvalidValue;
     wout->windows = (uint32_t)p.windows;
     wout->c = (uint32_t)p.c;
   }
-  const uint32_t W = (uint32_t)p.windows, B = p.buckets, L = p.seg_len;
+  const uint32_t Wj = (uint32_t)p.windows, B = p.buckets, L = p.seg_len;
+  const uint32_t W = Wj * jobs;  // windows of all jobs
+  if ((uint64_t)W * B >= (1ull << 31)) return cudaErrorInvalidValue;
   const uint32_t total = W * B;
   const uint32_t nblk = (total + 1023) / 1024;
-  const uint64_t entries = n * (uint64_t)W;
+  const uint64_t entries = n * (uint64_t)Wj;
   if (entries >= (1ull << 32)) return cudaErrorInvalidValue;  // entry offsets are 32-bit
   uint32_t *counts = nullptr, *offsets = nullptr, *cursor = nullptr, *bsums = nullptr, *list = nullptr;
   uint32_t *nsub = nullptr, *sub_off = nullptr, *sub2b = nullptr, *heavy = nullptr, *heavy_count = nullptr;
@@ -371,24 +400,24 @@ cudaError_t msm_run(const fe* d_scalars, const fe* d_bases, uint64_t n, fe* d_ou
     winsum = wout->d_winsum;  // caller's buffer, left for the host's Horner step
   else
     alloc((void**)&winsum, W * 128ull);
-  alloc((void**)&bases_rp, n * 64ull);
+  alloc((void**)&bases_rp, nbases * 64ull);
   if (e == cudaSuccess) {
     const double nd = (double)n;
     cudaMemsetAsync(counts, 0, total * 4ull, s);
     cudaMemsetAsync(heavy_count, 0, 4ull, s);
     const unsigned g = (unsigned)((n + 255) / 256);
     const unsigned gb = (total + 255) / 256;
-    msm_convert_bases_kernel<<<g, 256, 0, s>>>(d_bases, bases_rp, n);
+    msm_convert_bases_kernel<<<(unsigned)((nbases + 255) / 256), 256, 0, s>>>(d_bases, bases_rp, nbases);
     {
       ProfScope ps("msm_count", s, nd, nd * 32);
-      msm_count_kernel<<<g, 256, 0, s>>>(d_scalars, n, (uint32_t)p.c, W, counts);
+      msm_count_kernel<<<g, 256, 0, s>>>(d_scalars, n, (uint32_t)p.c, Wj, counts, job_off, jobs);
     }
     scan_block_kernel<<<nblk, 1024, 0, s>>>(counts, offsets, bsums, total);
     scan_sums_kernel<<<1, 1024, 0, s>>>(bsums, nblk, offsets + total);
     scan_add_kernel<<<nblk, 1024, 0, s>>>(offsets, cursor, bsums, total);
     {
       ProfScope ps("msm_scatter", s, nd, nd * 32 + (double)entries * 4);
-      msm_scatter_kernel<<<g, 256, 0, s>>>(d_scalars, n, (uint32_t)p.c, W, cursor, list);
+      msm_scatter_kernel<<<g, 256, 0, s>>>(d_scalars, n, (uint32_t)p.c, Wj, cursor, list, job_off, jobs);
     }
     msm_nsub_kernel<<<gb, 256, 0, s>>>(counts, nsub, total, sub_len);
     scan_block_kernel<<<nblk, 1024, 0, s>>>(nsub, sub_off, bsums, total);
@@ -421,6 +450,18 @@ cudaError_t msm_run(const fe* d_scalars, const fe* d_bases, uint64_t n, fe* d_ou
     if (ptr) cudaFreeAsync(ptr, s);
   if (launches) *launches = nl;
   return e;
+}
+}  // namespace
+
+cudaError_t msm_run(const fe* d_scalars, const fe* d_bases, uint64_t n, fe* d_out, cudaStream_t s, int c_override,
+                    uint64_t* launches, MsmWindowsOut* wout) {
+  return msm_run_impl(d_scalars, d_bases, n, d_out, s, c_override, launches, wout, nullptr, 1, n);
+}
+
+cudaError_t msm_run_multi(const fe* d_scalars, const fe* d_bases, const uint32_t* d_job_off, uint32_t jobs,
+                          uint64_t n_total, uint64_t max_n, cudaStream_t s, uint64_t* launches, MsmWindowsOut* wout) {
+  if (!wout || !wout->d_winsum || jobs == 0 || !d_job_off || n_total >= (1ull << 32)) return cudaErrorInvalidValue;
+  return msm_run_impl(d_scalars, d_bases, n_total, nullptr, s, 0, launches, wout, d_job_off, jobs, max_n);
 }
 
 }  // namespace zk

@@ -47,5 +47,14 @@ struct MsmWindowsOut {
 constexpr uint32_t MSM_MAX_WINDOWS = 64;  // c >= 4
 cudaError_t msm_run(const fe* d_scalars, const fe* d_bases_xy, uint64_t n, fe* d_out, cudaStream_t s,
                     int c_override = 0, uint64_t* launches = nullptr, MsmWindowsOut* wout = nullptr);
+// Several MSMs over one base array (the serving loop's jobs against resident
+// bases) in one pass: job j's scalars are [off[j], off[j+1]) of d_scalars
+// (d_job_off: jobs + 1 offsets in device memory, off[0] = 0), each against
+// bases [0, n_j); max_n = the largest n_j.  One window size (the plan of the
+// mean job size); job j's window sums land in windows [j W, (j + 1) W) of
+// wout->d_winsum (>= jobs * W * 4 elements), W = wout->windows on return.
+cudaError_t msm_run_multi(const fe* d_scalars, const fe* d_bases_xy, const uint32_t* d_job_off, uint32_t jobs,
+                          uint64_t n_total, uint64_t max_n, cudaStream_t s, uint64_t* launches,
+                          MsmWindowsOut* wout);
 
 }  // namespace zk

@@ -15,6 +15,7 @@
 #include <cstring>
 #include <deque>
 #include <memory>
+#include <map>
 #include <mutex>
 #include <thread>
 #include <unordered_map>
@@ -84,7 +85,8 @@ class Server {
     grid_ = ntt_batch_grid(device_);
     // one pinned mailbox per stream slot; a slot is reused only after the
     // wave that used it retired (waves retire in launch order)
-    slot_words_ = 2 + kMsmSlotWords * (uint64_t)max_wave_;
+    // per job: an MSM slot, plus room for the multi-MSM offsets (one word)
+    slot_words_ = 2 + (kMsmSlotWords + 1) * (uint64_t)max_wave_ + 2;
     ZK_TRY("cudaMallocHost(mailbox)", cudaMallocHost((void**)&mailbox_, kStreams * slot_words_ * 8));
     sched_ = std::thread([this] { sched_loop(); });
     comp_ = std::thread([this] { comp_loop(); });
@@ -258,8 +260,59 @@ class Server {
     std::vector<NttItem> items;
     std::vector<std::pair<JobRec*, fe*>> ntt_outputs;  // device result -> job
     std::vector<void*> frees_ntt, frees_msm;
+    // MSM jobs of this wave against the same resident bases run as one
+    // multi-MSM pass (one sort and bucket pass, one launch sequence);
+    // a lone MSM on its bases runs on its own
+    std::map<uint32_t, std::vector<JobRec*>> msm_groups;
+    for (JobRec* r : w.jobs)
+      if (r->job.kind == ZKGPU_KIND_MSM) msm_groups[r->job.bases_id].push_back(r);
+    for (auto& g : msm_groups) {
+      std::vector<JobRec*>& grp = g.second;
+      if (grp.size() < 2) continue;
+      const BaseSet& bs = bases_[g.first];
+      std::vector<uint32_t> off(grp.size() + 1, 0);
+      uint64_t max_n = 0;
+      for (size_t k = 0; k < grp.size(); k++) {
+        off[k + 1] = off[k] + (uint32_t)grp[k]->job.n;
+        max_n = std::max<uint64_t>(max_n, grp[k]->job.n);
+      }
+      const uint64_t n_total = off.back();
+      fe *ds = nullptr, *dwin = nullptr;
+      uint32_t* doff = nullptr;
+      if (ok(cudaMallocAsync((void**)&ds, std::max<uint64_t>(n_total, 1) * 32, w.s_msm)) &&
+          ok(cudaMallocAsync((void**)&dwin, grp.size() * MSM_MAX_WINDOWS * 128, w.s_msm)) &&
+          ok(cudaMallocAsync((void**)&doff, off.size() * 4, w.s_msm))) {
+        // offsets travel through the wave's pinned mailbox tail so the copy
+        // stays asynchronous
+        uint32_t* h_off = reinterpret_cast<uint32_t*>(next_msm_slot);
+        std::memcpy(h_off, off.data(), off.size() * 4);
+        next_msm_slot += (off.size() * 4 + 7) / 8;
+        ok(cudaMemcpyAsync(doff, h_off, off.size() * 4, cudaMemcpyHostToDevice, w.s_msm));
+        for (size_t k = 0; k < grp.size(); k++)
+          ok(cudaMemcpyAsync(ds + off[k], grp[k]->job.input, grp[k]->job.n * 32, cudaMemcpyHostToDevice,
+                             w.s_msm));
+        uint64_t nl = 0;
+        MsmWindowsOut wo;
+        wo.d_winsum = dwin;
+        if (ok(msm_run_multi(ds, bs.d, doff, (uint32_t)grp.size(), n_total, max_n, w.s_msm, &nl, &wo))) {
+          for (size_t k = 0; k < grp.size(); k++) {
+            JobRec* r = grp[k];
+            r->msm_out = next_msm_slot;
+            next_msm_slot += kMsmSlotWords;
+            r->msm_out[0] = wo.windows;
+            r->msm_out[1] = wo.c;
+            ok(cudaMemcpyAsync(r->msm_out + 2, dwin + (size_t)k * wo.windows * 4, wo.windows * 128ull,
+                               cudaMemcpyDeviceToHost, w.s_msm));
+          }
+        }
+      }
+      frees_msm.push_back(ds);
+      frees_msm.push_back(dwin);
+      frees_msm.push_back(doff);
+    }
     for (JobRec* r : w.jobs) {
       const zkgpu_job& j = r->job;
+      if (j.kind == ZKGPU_KIND_MSM && msm_groups[j.bases_id].size() >= 2) continue;  // ran above
       if (j.kind == ZKGPU_KIND_MSM) {
         // the window sums come back to the mailbox; the completion thread
         // does the Horner step on the host (host::fq::msm_combine_windows)
