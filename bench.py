@@ -488,7 +488,7 @@ def serving_trace(njobs: int, rate: float, seed: int = 99):
     return out
 
 
-def bench_serving(zk, torch, dev: int, njobs: int = 1000, rate: float = 2000.0, wave_jobs: int = 32):
+def bench_serving(zk, torch, dev: int, njobs: int = 1000, rate: float = 2000.0, wave_jobs: int = 64):
     """Serving loop (continuous batching) vs one call per job on the same GPU,
     same arrival trace; host buffers pinned, shared per size class (read-only
     inputs; outputs of identical jobs are identical)."""

@@ -242,9 +242,10 @@ uint64_t zkgpu_job_footprint(const zkgpu_job *job);
  * after admission (-1 = rejected).  Returns the peak bytes in use. */
 uint64_t zkgpu_admission_simulate(uint64_t budget, const uint64_t *footprints, uint32_t n, int32_t *admit_rounds);
 
-/* max_wave_jobs: jobs per scheduling wave (0 = 4096).  The server pins
- * 4 x (32 + 8216 x max_wave_jobs) bytes of host memory for its result
- * mailboxes (an MSM job's window sums come back there; 135 MB at 4096).
+/* max_wave_jobs: jobs per scheduling wave (0 = 256); up to 8 waves are on
+ * the GPU at once.  The server pins 8 x (32 + 8216 x max_wave_jobs) bytes of
+ * host memory for its result mailboxes (an MSM job's window sums come back
+ * there; 16.8 MB at 256).
  * MSM jobs of one wave against the same bases run as one multi-MSM pass. */
 int zkgpu_server_create(int device, uint64_t hbm_budget_bytes, uint32_t max_wave_jobs, void **server);
 /* upload a base set once (affine, 8 words per point); it stays resident */

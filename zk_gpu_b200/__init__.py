@@ -423,7 +423,7 @@ class Server:
     """Serving loop (continuous batching, HBM-budget admission) over the C ABI.
     Host buffers passed to submit() must stay alive until wait() returns."""
 
-    def __init__(self, device: int = 0, hbm_budget: int = 150 * 10**9, max_wave_jobs: int = 4096):
+    def __init__(self, device: int = 0, hbm_budget: int = 150 * 10**9, max_wave_jobs: int = 256):
         self.handle = ctypes.c_void_p()
         _check(lib().zkgpu_server_create(device, hbm_budget, max_wave_jobs, ctypes.byref(self.handle)),
                "server_create")

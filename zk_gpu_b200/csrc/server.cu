@@ -74,7 +74,7 @@ struct BaseSet {
 
 class Server {
  public:
-  Server(int dev, uint64_t budget, uint32_t max_wave) : device_(dev), adm_(budget), max_wave_(max_wave ? max_wave : 4096) {}
+  Server(int dev, uint64_t budget, uint32_t max_wave) : device_(dev), adm_(budget), max_wave_(max_wave ? max_wave : 256) {}
 
   int start() {
     ZK_TRY("cudaSetDevice", cudaSetDevice(device_));
@@ -185,7 +185,7 @@ class Server {
   }
 
  private:
-  static constexpr int kStreams = 4;
+  static constexpr int kStreams = 8;
   static constexpr int kEagerWaves = 2;
   // per MSM job in a wave's mailbox: window count, c, then the window sums
   static constexpr uint64_t kMsmSlotWords = 2 + 16 * (uint64_t)MSM_MAX_WINDOWS;
