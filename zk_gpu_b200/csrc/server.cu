@@ -266,9 +266,16 @@ class Server {
     std::map<uint32_t, std::vector<JobRec*>> msm_groups;
     for (JobRec* r : w.jobs)
       if (r->job.kind == ZKGPU_KIND_MSM) msm_groups[r->job.bases_id].push_back(r);
+    // merged passes keep their 32-bit entry offsets: at most 2^25 scalars
+    auto merged = [&](uint32_t bases_id) {
+      const std::vector<JobRec*>& grp = msm_groups[bases_id];
+      uint64_t tot = 0;
+      for (const JobRec* r : grp) tot += r->job.n;
+      return grp.size() >= 2 && tot <= (1ull << 25);
+    };
     for (auto& g : msm_groups) {
       std::vector<JobRec*>& grp = g.second;
-      if (grp.size() < 2) continue;
+      if (!merged(g.first)) continue;
       const BaseSet& bs = bases_[g.first];
       std::vector<uint32_t> off(grp.size() + 1, 0);
       uint64_t max_n = 0;
@@ -312,7 +319,7 @@ class Server {
     }
     for (JobRec* r : w.jobs) {
       const zkgpu_job& j = r->job;
-      if (j.kind == ZKGPU_KIND_MSM && msm_groups[j.bases_id].size() >= 2) continue;  // ran above
+      if (j.kind == ZKGPU_KIND_MSM && merged(j.bases_id)) continue;  // ran above
       if (j.kind == ZKGPU_KIND_MSM) {
         // the window sums come back to the mailbox; the completion thread
         // does the Horner step on the host (host::fq::msm_combine_windows)
