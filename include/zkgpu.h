@@ -131,12 +131,34 @@ int zkgpu_extended_to_coeff_dev(int device, const uint64_t *d_ext, uint32_t log_
  * allocation.  It calls no allocator: its scratch (ping-pong buffer and root
  * tables) is a static device array in the library sized for log_n <=
  * ZKGPU_STATIC_NTT_MAX_LOG (about 16.8 MB per GPU, held until process exit);
- * larger log_n returns ZKGPU_EINVAL.  The first call on a device resolves the
+ * larger log_n returns ZKGPU_EINVAL.  It always runs the built-in pass plan
+ * for log_n (the autotuner's choices are not consulted; results are the same,
+ * only the speed can differ).  The first call on a device resolves the
  * array's address, so make it before any stream capture starts.  All calls on
  * a device share the array: calls whose work overlaps on the GPU race and
  * must be serialised by the caller (one stream or events). */
 #define ZKGPU_STATIC_NTT_MAX_LOG 18
 int zkgpu_ntt_dev_static(int device, uint64_t *d_a, uint32_t log_n, const uint64_t omega[4], void *stream);
+/* Element-wise ops on device vectors of n Fr elements (extended-domain
+ * evaluations in halo2's quotient step: gates combined as h = h * y + e,
+ * polynomial products and sums).  No counterpart in the reference, whose
+ * only element-wise device op is distribute_powers (cuda/fft.cu:223-232);
+ * the operations restate halo2's Polynomial Mul / Add / Sub / scalar Mul on
+ * ExtendedLagrangeCoeff vectors.  d_out may alias d_a or d_b. */
+#define ZKGPU_EW_MUL 0u   /* out[i] = a[i] * b[i] */
+#define ZKGPU_EW_ADD 1u   /* out[i] = a[i] + b[i] */
+#define ZKGPU_EW_SUB 2u   /* out[i] = a[i] - b[i] */
+#define ZKGPU_EW_SCALE 3u /* out[i] = a[i] * c            (d_b unused) */
+#define ZKGPU_EW_AXPY 4u  /* out[i] = a[i] * c + b[i] */
+int zkgpu_ew_dev(int device, uint32_t op, uint64_t *d_out, const uint64_t *d_a, const uint64_t *d_b,
+                 const uint64_t c[4], uint64_t n, void *stream);
+/* halo2 EvaluationDomain::divide_by_vanishing_poly on device: d_ext holds the
+ * 2^log_ext evaluations on the coset g * <omega_ext>; element k is divided by
+ * t(X) = X^n - 1 there, t_k = g^n omega_ext^(n k) - 1, which takes only
+ * 2^(log_ext - log_n) <= 64 distinct values (inverted once on the host).
+ * ZKGPU_EINVAL when t vanishes somewhere on the coset. */
+int zkgpu_divide_by_vanishing_dev(int device, uint64_t *d_ext, uint32_t log_n, uint32_t log_ext, const uint64_t g[4],
+                                  const uint64_t omega_ext[4], void *stream);
 /* d_out_xyz receives the Jacobian sum (12 words, device memory) */
 int zkgpu_msm_dev(int device, const uint64_t *d_scalars, const uint64_t *d_bases_xy, uint64_t n, uint64_t *d_out_xyz,
                   void *stream);
@@ -232,6 +254,8 @@ typedef struct {
     uint64_t waves, batch_launches;
     uint64_t hbm_budget, hbm_used, hbm_peak;
     uint64_t pending, inflight;
+    uint64_t msm_merged_passes; /* multi-MSM passes (MSMs of one wave on shared bases) */
+    uint64_t msm_merged_jobs;   /* MSM jobs that ran inside such passes */
 } zkgpu_server_stats;
 
 /* device memory a job needs while in flight (bytes) */

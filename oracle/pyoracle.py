@@ -48,6 +48,10 @@ def lib():
             "zko_from_mont": (None, [i32, P, P]),
             "zko_field_mul_vec": (None, [i32, P, P, P, sz, i32]),
             "zko_field_dot": (None, [i32, P, P, P, sz, i32]),
+            "zko_field_add_vec": (None, [i32, P, P, P, sz, i32]),
+            "zko_field_sub_vec": (None, [i32, P, P, P, sz, i32]),
+            "zko_field_axpy_vec": (None, [i32, P, P, P, P, sz, i32]),
+            "zko_divide_by_vanishing": (i32, [P, u32, u32, P, P, i32]),
             "zko_rand_fr": (None, [P, sz, u64, sz, i32]),
             "zko_rand_fr_small": (None, [P, sz, u64, sz, i32, i32]),
             "zko_rand_bases": (None, [P, P, sz, u64, sz, i32]),
@@ -150,6 +154,45 @@ def mul_vec(a: np.ndarray, b: np.ndarray, fid=FR, threads=0) -> np.ndarray:
     b = np.ascontiguousarray(b, dtype=np.uint64)
     out = np.empty_like(a)
     lib().zko_field_mul_vec(fid, _p(out), _p(a), _p(b), a.shape[0], threads)
+    return out
+
+
+def add_vec(a: np.ndarray, b: np.ndarray, fid=FR, threads=0) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.uint64)
+    b = np.ascontiguousarray(b, dtype=np.uint64)
+    out = np.empty_like(a)
+    lib().zko_field_add_vec(fid, _p(out), _p(a), _p(b), a.shape[0], threads)
+    return out
+
+
+def sub_vec(a: np.ndarray, b: np.ndarray, fid=FR, threads=0) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.uint64)
+    b = np.ascontiguousarray(b, dtype=np.uint64)
+    out = np.empty_like(a)
+    lib().zko_field_sub_vec(fid, _p(out), _p(a), _p(b), a.shape[0], threads)
+    return out
+
+
+def axpy_vec(a: np.ndarray, c, b=None, fid=FR, threads=0) -> np.ndarray:
+    """a * c (+ b): c one element, a and b vectors"""
+    a = np.ascontiguousarray(a, dtype=np.uint64)
+    cc = _e(c)
+    out = np.empty_like(a)
+    bp = None
+    if b is not None:
+        b = np.ascontiguousarray(b, dtype=np.uint64)
+        bp = _p(b)
+    lib().zko_field_axpy_vec(fid, _p(out), _p(a), _p(cc), bp, a.shape[0], threads)
+    return out
+
+
+def divide_by_vanishing(ext: np.ndarray, log_n: int, log_ext: int, g, w_ext, threads: int = 0) -> np.ndarray:
+    """halo2 EvaluationDomain::divide_by_vanishing_poly over the coset g<w_ext>
+    (returns a new array; raises if X^n - 1 vanishes somewhere on the coset)"""
+    out = np.array(ext, dtype=np.uint64, copy=True, order="C")
+    gg, w = _e(g), _e(w_ext)
+    if lib().zko_divide_by_vanishing(_p(out), log_n, log_ext, _p(gg), _p(w), threads) != 0:
+        raise ValueError("X^n - 1 vanishes on this coset")
     return out
 
 

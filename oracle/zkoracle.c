@@ -164,6 +164,62 @@ void zko_field_mul_vec(int fid, u64 *out, const u64 *a, const u64 *b, size_t n, 
 
 static int nthreads(int threads) { return threads > 0 ? threads : omp_get_max_threads(); }
 
+/* Element-wise vector ops on extended-domain evaluations (halo2's quotient
+ * step combines polynomials in ExtendedLagrangeCoeff form this way:
+ * Polynomial Mul / Add / Sub and scalar Mul, halo2_proofs/src/poly.rs). */
+void zko_field_add_vec(int fid, u64 *out, const u64 *a, const u64 *b, size_t n, int threads) {
+    const field_t *F = fld(fid);
+#pragma omp parallel for num_threads(nthreads(threads)) schedule(static)
+    for (size_t i = 0; i < n; i++) fadd(F, out + 4 * i, a + 4 * i, b + 4 * i);
+}
+void zko_field_sub_vec(int fid, u64 *out, const u64 *a, const u64 *b, size_t n, int threads) {
+    const field_t *F = fld(fid);
+#pragma omp parallel for num_threads(nthreads(threads)) schedule(static)
+    for (size_t i = 0; i < n; i++) fsub(F, out + 4 * i, a + 4 * i, b + 4 * i);
+}
+/* out = a * c (+ b when b is not NULL), c one element */
+void zko_field_axpy_vec(int fid, u64 *out, const u64 *a, const u64 c[4], const u64 *b, size_t n, int threads) {
+    const field_t *F = fld(fid);
+#pragma omp parallel for num_threads(nthreads(threads)) schedule(static)
+    for (size_t i = 0; i < n; i++) {
+        u64 t[4];
+        fmul(F, t, a + 4 * i, c);
+        if (b) fadd(F, t, t, b + 4 * i);
+        cpy4(out + 4 * i, t);
+    }
+}
+
+/* halo2 EvaluationDomain::divide_by_vanishing_poly (halo2_proofs/src/poly/
+ * domain.rs, the external halo2 fork the reference's callers use): the
+ * vanishing polynomial t(X) = X^n - 1 takes only 2^(log_ext - log_n) distinct
+ * values on the coset g * <w_ext>, t_j = g^n * w_ext^(n j) - 1; they are
+ * inverted once and ext[k] is multiplied by 1 / t_(k mod 2^(log_ext-log_n)).
+ * Returns -1 (nothing changed) when some t_j is zero (g^n in <w_ext^n>). */
+int zko_divide_by_vanishing(u64 *ext, uint32_t log_n, uint32_t log_ext, const u64 g[4], const u64 omega_ext[4],
+                            int threads) {
+    if (log_ext < log_n || log_ext - log_n > 16) return -1;
+    const size_t n = (size_t)1 << log_n, N = (size_t)1 << log_ext, J = (size_t)1 << (log_ext - log_n);
+    u64 *tinv = (u64 *)malloc(sizeof(u64) * 4 * J);
+    u64 gn[4], step[4], cur[4];
+    fpow_u64(FR, gn, g, n);
+    fpow_u64(FR, step, omega_ext, n);
+    cpy4(cur, gn);
+    for (size_t j = 0; j < J; j++) {
+        u64 t[4];
+        fsub(FR, t, cur, FR->one);
+        if (is_zero4(t)) {
+            free(tinv);
+            return -1;
+        }
+        finv(FR, tinv + 4 * j, t);
+        fmul(FR, cur, cur, step);
+    }
+#pragma omp parallel for num_threads(nthreads(threads)) schedule(static)
+    for (size_t k = 0; k < N; k++) fmul(FR, ext + 4 * k, ext + 4 * k, tinv + 4 * (k & (J - 1)));
+    free(tinv);
+    return 0;
+}
+
 void zko_field_dot(int fid, u64 out[4], const u64 *a, const u64 *b, size_t n, int threads) {
     const field_t *F = fld(fid);
     int T = nthreads(threads);

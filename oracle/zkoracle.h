@@ -46,6 +46,15 @@ void zko_from_mont(int fid, uint64_t out[4], const uint64_t mont[4]);
 void zko_field_mul_vec(int fid, uint64_t *out, const uint64_t *a, const uint64_t *b, size_t n, int threads);
 /* out = sum_i a[i] * b[i] (Montgomery products, summed mod p) */
 void zko_field_dot(int fid, uint64_t out[4], const uint64_t *a, const uint64_t *b, size_t n, int threads);
+/* element-wise vector ops (extended-domain evaluations): out = a + b, a - b,
+ * a * c (+ b if b != NULL) */
+void zko_field_add_vec(int fid, uint64_t *out, const uint64_t *a, const uint64_t *b, size_t n, int threads);
+void zko_field_sub_vec(int fid, uint64_t *out, const uint64_t *a, const uint64_t *b, size_t n, int threads);
+void zko_field_axpy_vec(int fid, uint64_t *out, const uint64_t *a, const uint64_t c[4], const uint64_t *b, size_t n,
+                        int threads);
+/* halo2 divide_by_vanishing_poly on the coset g<w_ext>: ext[k] /= g^n w_ext^(n (k mod 2^(log_ext-log_n))) - 1 */
+int zko_divide_by_vanishing(uint64_t *ext, uint32_t log_n, uint32_t log_ext, const uint64_t g[4],
+                            const uint64_t omega_ext[4], int threads);
 
 /* ---- seeded synthetic inputs ------------------------------------------- */
 /* n uniform Fr elements in Montgomery form (each < r), counter-based so any

@@ -192,3 +192,37 @@ def test_small_scalars(oracle):
         assert oracle.from_mont(v) < 2**16
     pts, k = oracle.rand_bases(n, 2, with_dlog=True)
     assert np.array_equal(oracle.multiexp(s, pts), oracle.msm_by_dlog(s, k))
+
+
+def test_elementwise_vector_ops_vs_bigint(oracle):
+    n = 64
+    a, b = oracle.rand_fr(n, 21), oracle.rand_fr(n, 22)
+    c = oracle.to_mont(99991)
+    R = B.R_MOD
+
+    def val(x):
+        return oracle.from_mont(x)
+
+    s, d, m, ax = oracle.add_vec(a, b), oracle.sub_vec(a, b), oracle.mul_vec(a, b), oracle.axpy_vec(a, c, b)
+    for i in range(n):
+        x, y = val(a[i]), val(b[i])
+        assert val(s[i]) == (x + y) % R
+        assert val(d[i]) == (x - y) % R
+        assert val(m[i]) == x * y % R
+        assert val(ax[i]) == (x * 99991 + y) % R
+
+
+@pytest.mark.parametrize("k,e", [(2, 1), (4, 2), (5, 3)])
+def test_divide_by_vanishing_vs_direct_evaluation(oracle, k, e):
+    """ext[i] / ((g w^i)^n - 1), with the denominator evaluated directly in bigint"""
+    R = B.R_MOD
+    N = 1 << (k + e)
+    ext = oracle.rand_fr(N, 31 + k)
+    g = 7
+    w = oracle.from_mont(oracle.omega(k + e))
+    out = oracle.divide_by_vanishing(ext, k, k + e, oracle.to_mont(g), oracle.omega(k + e))
+    for i in range(N):
+        t = (pow(g * pow(w, i, R) % R, 1 << k, R) - 1) % R
+        assert oracle.from_mont(out[i]) == oracle.from_mont(ext[i]) * pow(t, -1, R) % R
+    with pytest.raises(ValueError):
+        oracle.divide_by_vanishing(ext, k, k + e, oracle.to_mont(1), oracle.omega(k + e))

@@ -4,8 +4,10 @@ It exists for callers that cannot allocate device memory — code running under
 CUDA stream capture, or inside a runtime that owns every device allocation —
 and keeps its scratch in a static device array inside libzkgpu.so.  Its
 output must equal the ordinary device entry point's (zkgpu_ntt_dev), bit for
-bit, on consecutive calls that reuse the shared array.  This file is collected
-last on purpose, and also passes when run alone in a fresh process.
+bit, on consecutive calls that reuse the shared array, and the CPU oracle's
+halo2 best_fft on the same input (so a fault shared by both device entry
+points cannot pass).  This file is collected last on purpose, and also passes
+when run alone in a fresh process.
 """
 import numpy as np
 import pytest
@@ -35,6 +37,8 @@ def test_static_matches_default_entry_on_consecutive_calls(zk, oracle, sizes):
         zk.ntt_dev(t_default, log_n, w, stream=stream)
         stream.synchronize()
         assert torch.equal(t_static, t_default), f"call {call}: log_n={log_n}"
+        want = oracle.best_fft(a, w, log_n)
+        assert np.array_equal(t_static.cpu().numpy().view(np.uint64), want), f"call {call}: oracle, log_n={log_n}"
 
 
 def test_static_rejects_oversize(zk, oracle):

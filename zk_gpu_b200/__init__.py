@@ -87,6 +87,8 @@ EXPORTS = {
     "zkgpu_tune_save": (_i32, [_i32, ctypes.c_char_p]),
     "zkgpu_tune_load": (_i32, [_i32, ctypes.c_char_p, P]),
     "zkgpu_extended_to_coeff_dev": (_i32, [_i32, P, _u32, P, _u64, P, P, P, P]),
+    "zkgpu_ew_dev": (_i32, [_i32, _u32, P, P, P, P, _u64, P]),
+    "zkgpu_divide_by_vanishing_dev": (_i32, [_i32, P, _u32, _u32, P, P, P]),
     "zkgpu_ntt_batch_create": (_i32, [_i32, P, _u32, P]),
     "zkgpu_ntt_batch_run": (_i32, [P, P]),
     "zkgpu_ntt_batch_check": (_i32, [P]),
@@ -310,6 +312,26 @@ def extended_to_coeff_dev(ext, out, log_ext: int, omega_ext_inv, ext_divisor, g_
            "extended_to_coeff_dev")
 
 
+EW_MUL, EW_ADD, EW_SUB, EW_SCALE, EW_AXPY = range(5)
+
+
+def ew_dev(op: int, out, a, b=None, c=None, stream=None):
+    """Element-wise op on CUDA tensors of shape (n, 4): out = a*b, a+b, a-b,
+    a*c or a*c + b (c one element); out may be a or b."""
+    dev = a.device.index
+    cc = _el(c) if c is not None else None
+    _check(lib().zkgpu_ew_dev(dev, op, _ptr(out), _ptr(a), _ptr(b) if b is not None else None,
+                              cc.ctypes.data if cc is not None else None, a.shape[0], _stream_ptr(stream)),
+           "ew_dev")
+
+
+def divide_by_vanishing_dev(ext, log_n: int, log_ext: int, g, omega_ext, stream=None):
+    """In place: ext[k] /= (g * omega_ext^k)^(2^log_n) - 1 (halo2 divide_by_vanishing_poly)."""
+    gg, we = _el(g), _el(omega_ext)
+    _check(lib().zkgpu_divide_by_vanishing_dev(ext.device.index, _ptr(ext), log_n, log_ext, gg.ctypes.data,
+                                               we.ctypes.data, _stream_ptr(stream)), "divide_by_vanishing_dev")
+
+
 JOB_COSET, JOB_SCALE = 1, 2
 
 
@@ -380,7 +402,7 @@ class Job(ctypes.Structure):
 class ServerStats(ctypes.Structure):
     _fields_ = [(k, ctypes.c_uint64) for k in ("submitted", "rejected", "completed", "failed", "waves",
                                                "batch_launches", "hbm_budget", "hbm_used", "hbm_peak", "pending",
-                                               "inflight")]
+                                               "inflight", "msm_merged_passes", "msm_merged_jobs")]
 
 
 def _set4(dst, v):

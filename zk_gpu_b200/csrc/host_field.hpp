@@ -92,6 +92,18 @@ inline Fr neg(const Fr& a) {
   }
   return r;
 }
+inline Fr add(const Fr& a, const Fr& b) {  // canonical inputs
+  Fr r;
+  unsigned __int128 c = 0;
+  for (int i = 0; i < 4; i++) {
+    c += (unsigned __int128)a.v[i] + b.v[i];
+    r.v[i] = (uint64_t)c;
+    c >>= 64;
+  }
+  if (geq(r.v, R_P)) sub_p(r.v);  // p < 2^254: no carry out of the top limb
+  return r;
+}
+inline Fr sub(const Fr& a, const Fr& b) { return add(a, neg(b)); }
 inline Fr pow_u64(Fr a, uint64_t e) {
   Fr r = one();
   while (e) {

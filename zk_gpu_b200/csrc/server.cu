@@ -10,6 +10,7 @@
 // budget (which wakes the scheduler: new arrivals are admitted while earlier
 // waves still run, so their work overlaps on the device) and wakes waiters.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -182,6 +183,8 @@ class Server {
     o->hbm_peak = peak_;
     o->pending = adm_.pending();
     o->inflight = inflight_jobs_;
+    o->msm_merged_passes = merged_passes_;
+    o->msm_merged_jobs = merged_jobs_;
   }
 
  private:
@@ -302,6 +305,8 @@ class Server {
         MsmWindowsOut wo;
         wo.d_winsum = dwin;
         if (ok(msm_run_multi(ds, bs.d, doff, (uint32_t)grp.size(), n_total, max_n, w.s_msm, &nl, &wo))) {
+          merged_passes_++;
+          merged_jobs_ += grp.size();
           for (size_t k = 0; k < grp.size(); k++) {
             JobRec* r = grp[k];
             r->msm_out = next_msm_slot;
@@ -519,6 +524,7 @@ class Server {
   bool stop_ = false;
   uint64_t next_ticket_ = 1, submitted_ = 0, rejected_ = 0, completed_ = 0, failed_ = 0, waves_ = 0;
   uint64_t batch_launches_ = 0, peak_ = 0, inflight_jobs_ = 0, retired_gen_ = 0;
+  std::atomic<uint64_t> merged_passes_{0}, merged_jobs_{0};
   int waves_inflight_ = 0;
   uint64_t* mailbox_ = nullptr;
   uint64_t slot_words_ = 0;

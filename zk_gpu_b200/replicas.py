@@ -90,48 +90,135 @@ def place_job(footprint: int, running: list, used: list, capacity: list) -> int:
 
 
 class MultiGpuServer:
-    """One serving loop (zk.Server) per local GPU, jobs placed by place_job.
-    Bases added here are made resident on every device."""
+    """One serving loop (zk.Server) per local GPU; each job goes to a device
+    chosen by place_job, the role of GpuLock::acquire_gpu / release_gpu
+    (src/gpulock.rs:133-226).
 
-    def __init__(self, devices: list, hbm_budget: int = 150 * 10**9, max_wave_jobs: int = 4096):
-        from . import Server
+    Two ledgers exist on purpose, at two levels.  This object's per-device
+    counters (bytes placed, jobs running) decide WHICH device takes a job,
+    before the job is queued anywhere, as GpuLock's mem_used / running_tasks
+    do.  Each device's Server then enforces its HBM budget at execution time
+    (its admission queue also holds the resident bases, which the placement
+    ledger does not see) and decides WHEN the job starts.
+
+    Thread safety: every counter is read and written under one condition
+    variable.  Release happens on completion, not in wait(): a reaper thread
+    per device waits for that device's jobs in submission order (a Server
+    retires jobs in admission order, which is submission order) and gives
+    their bytes back at once, so a job that is never waited on does not hold
+    its budget; its result stays available to wait() until taken.
+    submit() blocks while no device has room (the reference's acquire_gpu
+    blocks the same way), up to an optional timeout.
+
+    Bases added here are made resident on every device.  `server_factory`
+    (device -> server object with submit / wait / close / add_bases) lets
+    tests run the placement logic against stand-in servers without a GPU."""
+
+    def __init__(self, devices: list, hbm_budget: int = 150 * 10**9, max_wave_jobs: int = 256,
+                 server_factory=None, footprint=None):
+        import collections
+        import threading
+        if server_factory is None:
+            from . import Server
+
+            def server_factory(d):
+                return Server(d, hbm_budget, max_wave_jobs)
+        if footprint is None:
+            from . import job_footprint as footprint
+        self._footprint = footprint
         self.devices = list(devices)
-        self.servers = [Server(d, hbm_budget, max_wave_jobs) for d in self.devices]
+        self.servers = [server_factory(d) for d in self.devices]
         self.capacity = [hbm_budget] * len(self.devices)
         self.used = [0] * len(self.devices)
         self.running = [0] * len(self.devices)
-        self._where = {}
+        self.placed = [0] * len(self.devices)
+        self._cv = threading.Condition()
+        self._where = {}       # ticket -> (device index, server ticket, bytes)
+        self._results = {}     # ticket -> (exception or None, latency ms)
+        self._queues = [collections.deque() for _ in self.devices]
         self._next = 0
+        self._closing = False
+        self._reapers = [threading.Thread(target=self._reap, args=(i,), daemon=True)
+                         for i in range(len(self.devices))]
+        for t in self._reapers:
+            t.start()
 
     def add_bases(self, bases) -> int:
         ids = {s.add_bases(bases) for s in self.servers}
         assert len(ids) == 1, "base ids diverged across devices"
         return ids.pop()
 
-    def submit(self, job, keep=None) -> int:
-        """Returns a ticket; raises RuntimeError when no device has room
-        (the caller waits for a completion and retries)."""
-        from . import job_footprint
-        fp = job_footprint(job)
-        d = place_job(fp, self.running, self.used, self.capacity)
-        if d < 0:
-            raise RuntimeError("no device has room for this job now")
-        t = self.servers[d].submit(job, keep)
-        self.used[d] += fp
-        self.running[d] += 1
-        ticket = self._next
-        self._next += 1
-        self._where[ticket] = (d, t, fp)
+    def submit(self, job, keep=None, timeout_s: float | None = None) -> int:
+        """Place the job and queue it on that device's server; returns a
+        ticket.  Blocks while no device has room; raises TimeoutError after
+        timeout_s, and ValueError for a job larger than every device."""
+        fp = int(self._footprint(job))
+        if fp > max(self.capacity):
+            raise ValueError(f"job footprint {fp} exceeds every device's budget")
+        with self._cv:
+            if self._closing:
+                raise RuntimeError("MultiGpuServer is closed")
+            ok = self._cv.wait_for(lambda: place_job(fp, self.running, self.used, self.capacity) >= 0,
+                                   timeout=timeout_s)
+            if not ok:
+                raise TimeoutError("no device had room for the job in time")
+            d = place_job(fp, self.running, self.used, self.capacity)
+            t = self.servers[d].submit(job, keep)  # non-blocking; raises on rejection
+            self.used[d] += fp
+            self.running[d] += 1
+            self.placed[d] += 1
+            ticket = self._next
+            self._next += 1
+            self._where[ticket] = (d, t, fp)
+            self._queues[d].append(ticket)
+            self._cv.notify_all()
         return ticket
 
+    def _reap(self, d: int):
+        while True:
+            with self._cv:
+                self._cv.wait_for(lambda: self._queues[d] or self._closing)
+                if not self._queues[d]:
+                    return
+                ticket = self._queues[d][0]
+                _, t, fp = self._where[ticket]
+            try:
+                res = (None, self.servers[d].wait(t))
+            except Exception as ex:  # the job failed on its device: report it to wait()
+                res = (ex, None)
+            with self._cv:
+                self._queues[d].popleft()
+                del self._where[ticket]
+                self.used[d] -= fp
+                self.running[d] -= 1
+                self._results[ticket] = res
+                self._cv.notify_all()
+
     def wait(self, ticket: int, timeout_ms: int = 0) -> float:
-        d, t, fp = self._where.pop(ticket)
-        try:
-            return self.servers[d].wait(t, timeout_ms)
-        finally:
-            self.used[d] -= fp
-            self.running[d] -= 1
+        """Latency (ms) of a job, once it completed; re-raises its failure."""
+        with self._cv:
+            if ticket not in self._results and ticket not in self._where:
+                raise KeyError(f"unknown ticket {ticket}")
+            ok = self._cv.wait_for(lambda: ticket in self._results,
+                                   timeout=None if timeout_ms == 0 else timeout_ms / 1e3)
+            if not ok:
+                raise TimeoutError(f"job {ticket} still running")
+            ex, lat = self._results.pop(ticket)
+        if ex is not None:
+            raise ex
+        return lat
+
+    def counters(self) -> dict:
+        with self._cv:
+            return {"used": list(self.used), "running": list(self.running), "placed": list(self.placed),
+                    "in_flight": len(self._where)}
 
     def close(self):
+        """Finish the jobs in flight, stop the reapers, close the servers."""
+        with self._cv:
+            self._closing = True
+            self._cv.notify_all()
+        for t in self._reapers:
+            t.join()
         for s in self.servers:
             s.close()
