@@ -151,3 +151,26 @@ def test_msm_host_and_device_horner_agree(zk, oracle, n):
     assert np.array_equal(affine_of(host), oracle.g1_normalize(jac))
     if n <= 1 << 14:
         assert np.array_equal(affine_of(host), oracle.multiexp(s, pts))
+
+
+@pytest.mark.parametrize("n_pos,n_neg", [(2048, 2048), (3000, 1096), (1, 1), (517, 0)])
+def test_msm_in_bucket_doubling_and_cancellation(zk, oracle, n_pos, n_neg):
+    """All scalars equal, so each window has a single bucket holding copies
+    of P and -P in the order the sort left them: the pairwise (affine) bucket
+    sums meet P + P (doubling), P + (-P) (identity) and identity operands."""
+    pts, k = oracle.rand_bases(1, 77, with_dlog=True)
+    q = zk.FQ_MODULUS
+    p = pts[0]
+    neg = p.copy()
+    neg[4:] = oracle.to_mont((q - oracle.from_mont(p[4:], oracle.FQ)) % q, oracle.FQ)
+    n = n_pos + n_neg
+    rng = np.random.default_rng(n_pos * 7 + n_neg)
+    order = rng.permutation(n)
+    bases = np.empty((n, 8), np.uint64)
+    bases[order[:n_pos]] = p
+    bases[order[n_pos:]] = neg
+    s = np.tile(oracle.to_mont(0xBEEF), (n, 1))
+    # expected: 0xBEEF * (n_pos - n_neg) * k * G
+    kk = oracle.mul(oracle.to_mont((n_pos - n_neg) % B.R_MOD), k[0])
+    want = oracle.msm_by_dlog(s[:1], kk.reshape(1, 4))
+    assert np.array_equal(affine_of(zk.msm(s, bases)), want)

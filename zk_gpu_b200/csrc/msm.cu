@@ -7,7 +7,7 @@
 
 namespace zk {
 
-MsmPlan make_msm_plan(uint64_t n, int c_override) {
+MsmPlan make_msm_plan(uint64_t n, int c_override, int device) {
   MsmPlan p;
   int lg = 1;
   while ((1ull << lg) < n) lg++;
@@ -15,8 +15,8 @@ MsmPlan make_msm_plan(uint64_t n, int c_override) {
   if (c < 4) c = 4;
   if (c > 16) c = 16;
   if (c_override == 0) {  // the autotuner's choice for this device and size, if any
-    int dev = 0;
-    if (cudaGetDevice(&dev) == cudaSuccess) c_override = tuned_msm_window(dev, lg);
+    int dev = device;
+    if (dev >= 0 || cudaGetDevice(&dev) == cudaSuccess) c_override = tuned_msm_window(dev, lg);
   }
   if (c_override >= 3 && c_override <= 20) c = c_override;
   p.c = c;
@@ -151,102 +151,298 @@ __global__ void scan_add_kernel(uint32_t* out, uint32_t* cursor, const uint32_t*
   cursor[i] = v;
 }
 
-// Buckets are split into sub-buckets of at most SUB entries, one thread
-// each, so a bucket that collects a large share of the points (skewed
-// scalars, e.g. many small ones all carrying into the same digit) is summed
-// by many threads instead of one.
-constexpr uint32_t SUB_MAX = 64;      // entries per sub-bucket (large MSMs)
-constexpr uint32_t SUB_MIN = 16;      // small MSMs: shorter chains, more threads
-constexpr uint32_t SEQ_MAX = 16;      // sub-sums a bucket combines in one thread
+// ---------------------------------------------------------------------------
+// Batch-affine bucket accumulation.
+//
+// Every bucket's points are summed by pairwise AFFINE additions in rounds:
+// round r replaces the c points of a bucket by ceil(c / 2) points (pair sums,
+// plus the odd last point carried).  An affine addition P + Q needs
+// 1 / (x_Q - x_P); the inverses of a whole round come from Montgomery's
+// trick in two levels:
+//   prefix  : each thread task owns BA_K consecutive pair sums and chains
+//             the products of their denominators (stored, 1 product each);
+//   invert  : each inversion thread takes BA_G task products, chains them,
+//             inverts the chain's product once (Fermat) and walks back;
+//   apply   : each task walks its chain back (2 products per sum) and
+//             finishes the additions (lambda, lambda^2, lambda (x1 - x3):
+//             3 products).
+// That is about 6 + 331 / (BA_K BA_G) + 3 / BA_K ~ 6.8 Fq products per
+// point addition (the XYZZ mixed addition costs 10), with every inversion
+// amortised over 512 additions and no serial block-wide step.  Equal x
+// (P = Q: doubling, denominator 2y; P = -Q: identity) and the identity
+// (x = 0: no BN254 point has x = 0, as 3 is not a square mod q) are handled
+// per sum.  A bucket reaching one point writes it to `fin`; after the last
+// round a tail kernel folds what remains (skewed buckets) with XYZZ mixed
+// additions and writes every bucket as XYZZ for the reduction.
+// ---------------------------------------------------------------------------
+constexpr uint32_t BA_K = 16;  // pair sums per task (one chain of products)
+constexpr uint32_t BA_G = 32;  // task products per inversion
 
-__global__ void msm_nsub_kernel(const uint32_t* counts, uint32_t* nsub, uint32_t total, uint32_t sub_len) {
-  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b < total) nsub[b] = (counts[b] + sub_len - 1) / sub_len;
+__device__ __forceinline__ void fq_one_rp(uint32_t r[8]) { set_one_rp<FqP>(r); }
+
+// a^(q-2) = a^-1 (a != 0), R' form, lazy in, canonical out; 4-bit fixed
+// windows: 254 squarings + 63 products + 14 for the table
+__device__ __noinline__ void fq_inv_rp_w4(uint32_t r[8], const uint32_t a[8]) {
+  uint32_t tab[16][8];
+  fq_one_rp(tab[0]);
+  cpy(tab[1], a);
+  for (int i = 2; i < 16; i++) qmul(tab[i], tab[i - 1], a);
+  const uint32_t e[8] = {FqP::P0 - 2u, FqP::P1, FqP::P2, FqP::P3, FqP::P4, FqP::P5, FqP::P6, FqP::P7};
+  uint32_t acc[8];
+  cpy(acc, tab[e[7] >> 28]);
+  for (int nib = 62; nib >= 0; nib--) {
+    qsqr(acc, acc);
+    qsqr(acc, acc);
+    qsqr(acc, acc);
+    qsqr(acc, acc);
+    const uint32_t d = (e[nib >> 3] >> (4 * (nib & 7))) & 15u;
+    if (d) qmul(acc, acc, tab[d]);
+  }
+  reduce_once<FqP>(r, acc);
 }
 
-__global__ void msm_submap_kernel(const uint32_t* nsub, const uint32_t* sub_off, uint32_t* sub2b, uint32_t total) {
-  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= total) return;
-  const uint32_t k = nsub[b], o = sub_off[b];
-  for (uint32_t j = 0; j < k; j++) sub2b[o + j] = b;
+// the point at position pos of a round's input: round 0 gathers the signed
+// base named by the sorted entry list, later rounds read their own buffer
+template <bool FIRST>
+__device__ __forceinline__ void ba_load(aff_t& p, const fe* src, const uint32_t* list, uint32_t pos) {
+  if (FIRST) {
+    const uint32_t e = list[pos];
+    ld_aff(p, src + 2 * (uint64_t)(e & 0x7fffffffu));
+    if ((e & 0x80000000u) && !is_zero(p.x)) {
+      uint32_t z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      sub<FqP>(p.y, z, p.y);
+    }
+  } else {
+    ld_aff(p, src + 2 * (uint64_t)pos);
+  }
+}
+template <bool FIRST>
+__device__ __forceinline__ void ba_load_x(uint32_t x[8], const fe* src, const uint32_t* list, uint32_t pos) {
+  if (FIRST)
+    ld_fe(x, src + 2 * (uint64_t)(list[pos] & 0x7fffffffu));
+  else
+    ld_fe(x, src + 2 * (uint64_t)pos);
 }
 
-// One thread per sub-bucket: sum of its (signed) points.
-__global__ void __launch_bounds__(256) msm_subbucket_kernel(const uint32_t* list, const uint32_t* offsets,
-                                                            const uint32_t* counts, const uint32_t* sub_off,
-                                                            const uint32_t* sub2b, const uint32_t* total_sub,
-                                                            const fe* bases, fe* subres, uint32_t sub_len) {
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= *total_sub) return;
-  const uint32_t b = sub2b[s];
-  const uint32_t j = s - sub_off[b];
-  const uint32_t beg = offsets[b] + j * sub_len;
-  const uint32_t end = min(offsets[b] + counts[b], beg + sub_len);
+// denominator of one pair sum (R' one when no inversion is needed: a carried
+// point, an identity operand, or P = -Q)
+template <bool FIRST>
+__device__ __forceinline__ void ba_denominator(uint32_t d[8], const fe* src, const uint32_t* list, uint32_t i0,
+                                               bool has2) {
+  if (has2) {
+    uint32_t x1[8], x2[8];
+    ba_load_x<FIRST>(x1, src, list, i0);
+    ba_load_x<FIRST>(x2, src, list, i0 + 1);
+    if (!is_zero(x1) && !is_zero(x2)) {
+      if (!eq(x1, x2)) {
+        sub<FqP>(d, x2, x1);
+        return;
+      }
+      aff_t p, q;
+      ba_load<FIRST>(p, src, list, i0);
+      ba_load<FIRST>(q, src, list, i0 + 1);
+      if (eq(p.y, q.y)) {
+        add<FqP>(d, p.y, p.y);
+        return;
+      }
+    }
+  }
+  fq_one_rp(d);
+}
+
+// largest bucket b < T with joff[b] <= q (joff: exclusive scan of jobs)
+__device__ __forceinline__ uint32_t ba_bucket_of(const uint32_t* joff, uint32_t T, uint32_t q) {
+  uint32_t lo = 0, hi = T;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (joff[mid] <= q) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// buckets with at most one entry are final before any round; every count
+// is copied for the rounds
+__global__ void ba_setup_kernel(const uint32_t* counts, const uint32_t* offsets, const uint32_t* list,
+                                const fe* bases, uint32_t* cnt, fe* fin, uint32_t T) {
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= T) return;
+  const uint32_t c = counts[b];
+  cnt[b] = c;
+  if (c == 1) {
+    aff_t p;
+    ba_load<true>(p, bases, list, offsets[b]);
+    st_fe(fin + 2 * (uint64_t)b, p.x);
+    st_fe(fin + 2 * (uint64_t)b + 1, p.y);
+  } else if (c == 0) {
+    uint32_t z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    st_fe(fin + 2 * (uint64_t)b, z);
+    st_fe(fin + 2 * (uint64_t)b + 1, z);
+  }
+}
+
+__global__ void ba_jobs_kernel(const uint32_t* cnt, uint32_t* cprev, uint32_t* np, uint32_t T) {
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= T) return;
+  const uint32_t c = cnt[b];
+  cprev[b] = c;
+  np[b] = c >= 2 ? (c + 1) / 2 : 0;
+}
+
+// prefix: task t covers jobs [t K, t K + K) of the round (J = joff[T])
+template <bool FIRST>
+__global__ void __launch_bounds__(256) ba_prefix_kernel(const fe* src, const uint32_t* list, const uint32_t* in_off,
+                                                        const uint32_t* cprev, const uint32_t* joff,
+                                                        const uint32_t* np, uint32_t T, fe* pre, fe* tot) {
+  const uint32_t J = joff[T];
+  const uint32_t tasks = (J + BA_K - 1) / BA_K;
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < tasks; t += gridDim.x * blockDim.x) {
+    const uint32_t q0 = t * BA_K, q1 = min(q0 + BA_K, J);
+    uint32_t b = ba_bucket_of(joff, T, q0);
+    uint32_t acc[8];
+    for (uint32_t q = q0; q < q1; q++) {
+      if (q - joff[b] >= np[b]) b = ba_bucket_of(joff, T, q);
+      const uint32_t j = q - joff[b];
+      uint32_t d[8];
+      ba_denominator<FIRST>(d, src, list, in_off[b] + 2 * j, 2 * j + 1 < cprev[b]);
+      if (q == q0)
+        cpy(acc, d);
+      else
+        qmul(acc, acc, d);
+      st_fe(pre + q, acc);
+    }
+    st_fe(tot + t, acc);
+  }
+}
+
+// invert: thread s turns tot[s G .. s G + G) into their inverses
+__global__ void __launch_bounds__(128) ba_invert_kernel(fe* tot, fe* tpre, const uint32_t* joff, uint32_t T) {
+  const uint32_t J = joff[T];
+  const uint32_t tasks = (J + BA_K - 1) / BA_K;
+  const uint32_t groups = (tasks + BA_G - 1) / BA_G;
+  for (uint32_t sgi = blockIdx.x * blockDim.x + threadIdx.x; sgi < groups; sgi += gridDim.x * blockDim.x) {
+    const uint32_t i0 = sgi * BA_G, i1 = min(i0 + BA_G, tasks);
+    uint32_t acc[8], v[8];
+    ld_fe(acc, tot + i0);
+    st_fe(tpre + i0, acc);
+    for (uint32_t i = i0 + 1; i < i1; i++) {
+      ld_fe(v, tot + i);
+      qmul(acc, acc, v);
+      st_fe(tpre + i, acc);
+    }
+    uint32_t inv[8];
+    fq_inv_rp_w4(inv, acc);
+    for (uint32_t i = i1 - 1; i > i0; i--) {
+      uint32_t p[8], it[8];
+      ld_fe(p, tpre + i - 1);
+      ld_fe(v, tot + i);
+      qmul(it, inv, p);
+      qmul(inv, inv, v);
+      st_fe(tot + i, it);
+    }
+    st_fe(tot + i0, inv);
+  }
+}
+
+// apply: walk each task's chain back and finish its pair sums
+template <bool FIRST>
+__global__ void __launch_bounds__(256) ba_apply_kernel(const fe* src, const uint32_t* list, const uint32_t* in_off,
+                                                       const uint32_t* cprev, const uint32_t* joff,
+                                                       const uint32_t* np, uint32_t T, const fe* pre, const fe* tot,
+                                                       fe* dst, fe* fin, uint32_t* cnt) {
+  const uint32_t J = joff[T];
+  const uint32_t tasks = (J + BA_K - 1) / BA_K;
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < tasks; t += gridDim.x * blockDim.x) {
+    const uint32_t q0 = t * BA_K, q1 = min(q0 + BA_K, J);
+    uint32_t inv_run[8];
+    ld_fe(inv_run, tot + t);
+    uint32_t b = ba_bucket_of(joff, T, q1 - 1);
+    for (uint32_t q = q1; q-- > q0;) {
+      if (q < joff[b]) b = ba_bucket_of(joff, T, q);
+      const uint32_t j = q - joff[b], c = cprev[b];
+      const uint32_t i0 = in_off[b] + 2 * j;
+      const bool has2 = 2 * j + 1 < c;
+      aff_t P, Q, out;
+      ba_load<FIRST>(P, src, list, i0);
+      if (has2) ba_load<FIRST>(Q, src, list, i0 + 1);
+      // the same denominator the prefix pass chained (ba_denominator)
+      uint32_t d[8];
+      int kind = 0;  // 0: no inversion, 1: addition, 2: doubling
+      if (has2 && !is_zero(P.x) && !is_zero(Q.x)) {
+        if (!eq(P.x, Q.x)) {
+          sub<FqP>(d, Q.x, P.x);
+          kind = 1;
+        } else if (eq(P.y, Q.y)) {
+          add<FqP>(d, P.y, P.y);
+          kind = 2;
+        }
+      }
+      if (kind == 0) fq_one_rp(d);
+      uint32_t inv_d[8];
+      if (q > q0) {
+        uint32_t p[8];
+        ld_fe(p, pre + q - 1);
+        qmul(inv_d, inv_run, p);
+        qmul(inv_run, inv_run, d);
+      } else {
+        cpy(inv_d, inv_run);
+      }
+      if (!has2 || is_zero(Q.x)) {
+        out = P;
+      } else if (is_zero(P.x)) {
+        out = Q;
+      } else if (kind == 0) {  // P = -Q
+        set_zero(out.x);
+        set_zero(out.y);
+      } else {
+        uint32_t lam[8], t1[8];
+        if (kind == 1) {
+          sub<FqP>(t1, Q.y, P.y);
+        } else {  // doubling: 3 x^2 / (2 y)
+          qsqr(t1, P.x);
+          uint32_t t2[8];
+          add_lazy<FqP>(t2, t1, t1);
+          add_lazy<FqP>(t1, t2, t1);
+        }
+        qmul(lam, t1, inv_d);
+        qsqr(t1, lam);
+        qsub(t1, t1, P.x);
+        qsub(out.x, t1, Q.x);  // Q.x = P.x when doubling
+        reduce_once<FqP>(out.x, out.x);
+        qsub(t1, P.x, out.x);
+        qmul(t1, lam, t1);
+        qsub(out.y, t1, P.y);
+        reduce_once<FqP>(out.y, out.y);
+      }
+      const uint32_t nb = np[b];
+      fe* o = nb == 1 ? fin + 2 * (uint64_t)b : dst + 2 * (uint64_t)(joff[b] + j);
+      st_fe(o, out.x);
+      st_fe(o + 1, out.y);
+      if (j == 0) cnt[b] = nb;
+    }
+  }
+}
+
+// tail: every bucket to XYZZ; buckets still holding more than one point
+// (skewed inputs past the last round) are folded with mixed additions
+__global__ void ba_tail_kernel(const uint32_t* cnt, const uint32_t* in_off, const fe* src, const fe* fin,
+                               fe* buckets, uint32_t T) {
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= T) return;
+  const uint32_t c = cnt[b];
   xyzz_t acc;
   xyzz_set_inf(acc);
-  for (uint32_t k = beg; k < end; k++) {
-    const uint32_t e = list[k];
-    aff_t q;
-    ld_aff(q, bases + 2 * (uint64_t)(e & 0x7fffffffu));
-    if (aff_is_inf(q)) continue;
-    if (e & 0x80000000u) {
-      uint32_t z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-      sub<FqP>(q.y, z, q.y);
+  aff_t p;
+  if (c <= 1) {
+    ld_aff(p, fin + 2 * (uint64_t)b);
+    xyzz_from_aff(acc, p);  // (0, 0) -> identity
+  } else {
+    const uint32_t o = in_off[b];
+    for (uint32_t i = 0; i < c; i++) {
+      ld_aff(p, src + 2 * (uint64_t)(o + i));
+      xyzz_madd(acc, p);
     }
-    xyzz_madd(acc, q);
-  }
-  st_xyzz(subres + 4 * (uint64_t)s, acc);
-}
-
-// One thread per bucket: combine its sub-sums when there are few; queue the
-// bucket for the block-wide reduction when there are many.
-__global__ void msm_bucket_final_kernel(const uint32_t* nsub, const uint32_t* sub_off, const fe* subres, fe* buckets,
-                                        uint32_t* heavy, uint32_t* heavy_count, uint32_t total) {
-  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= total) return;
-  const uint32_t k = nsub[b], o = sub_off[b];
-  if (k > SEQ_MAX) {
-    heavy[atomicAdd(heavy_count, 1u)] = b;
-    return;
-  }
-  xyzz_t acc, t;
-  xyzz_set_inf(acc);
-  for (uint32_t j = 0; j < k; j++) {
-    ld_xyzz(t, subres + 4 * (uint64_t)(o + j));
-    xyzz_add(acc, t);
   }
   st_xyzz(buckets + 4 * (uint64_t)b, acc);
-}
-
-// One block per queued heavy bucket: strided partial sums, then a tree.
-__global__ void __launch_bounds__(256) msm_heavy_kernel(const uint32_t* nsub, const uint32_t* sub_off,
-                                                        const fe* subres, fe* buckets, const uint32_t* heavy,
-                                                        const uint32_t* heavy_count) {
-  __shared__ fe sh[256 * 4];
-  if (blockIdx.x >= *heavy_count) return;
-  const uint32_t b = heavy[blockIdx.x];
-  const uint32_t k = nsub[b], o = sub_off[b];
-  xyzz_t acc, t;
-  xyzz_set_inf(acc);
-  for (uint32_t j = threadIdx.x; j < k; j += blockDim.x) {
-    ld_xyzz(t, subres + 4 * (uint64_t)(o + j));
-    xyzz_add(acc, t);
-  }
-  st_xyzz(sh + 4 * threadIdx.x, acc);
-  __syncthreads();
-  for (uint32_t half = blockDim.x / 2; half > 0; half >>= 1) {
-    if (threadIdx.x < half) {
-      ld_xyzz(acc, sh + 4 * threadIdx.x);
-      ld_xyzz(t, sh + 4 * (threadIdx.x + half));
-      xyzz_add(acc, t);
-      st_xyzz(sh + 4 * threadIdx.x, acc);
-    }
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) {
-    ld_xyzz(acc, sh);
-    st_xyzz(buckets + 4 * (uint64_t)b, acc);
-  }
 }
 
 // Per (window, segment): running sums over the segment's buckets, top down,
@@ -337,12 +533,71 @@ __global__ void zero_out_kernel(fe* out) {
 }
 
 namespace {
+// Buffer sizes of one MSM pass (msm_run_impl allocates exactly these;
+// msm_scratch_bytes reports them for admission).
+struct MsmLayout {
+  MsmPlan p;
+  uint32_t Wj = 0, W = 0, B = 0, L = 0, T = 0, nblk = 0, segs = 0, rounds = 0;
+  uint64_t E = 0;                // entries (point-window pairs), upper bound
+  uint64_t jb[2] = {0, 0};       // pair sums of rounds 0 and 1, upper bounds
+  uint64_t tasks0 = 0;
+  bool ok = false;
+  uint64_t bytes(bool own_winsum, uint64_t nbases_convert) const {
+    const uint64_t T1 = T + 1ull;
+    uint64_t b = 0;
+    b += T * 4ull * 2 + T1 * 4 + (nblk + 1ull) * 4 + E * 4;        // counts, cursor, offsets, bsums, list
+    b += T * 4ull * 3 + T1 * 4 * 2 + T * 64ull;                   // cnt, cprev, np, joff x2, fin
+    b += jb[0] * 64 + (rounds > 1 ? jb[1] * 64 : 0) + jb[0] * 32;  // round buffers, prefixes
+    b += tasks0 * 32 * 2;                                         // task products, their prefixes
+    b += T * 128ull + segs * 128ull + (own_winsum ? W * 128ull : 0);
+    b += nbases_convert * 64;
+    return b + 24 * 256;  // pool granularity per allocation
+  }
+};
+
+MsmLayout msm_layout(uint64_t n, uint32_t jobs, int c_override, int device = -1) {
+  MsmLayout l;
+  if (jobs == 0) jobs = 1;
+  l.p = make_msm_plan((n + jobs - 1) / jobs, c_override, device);  // one window size: the mean job size's plan
+  l.Wj = (uint32_t)l.p.windows;
+  l.B = l.p.buckets;
+  l.L = l.p.seg_len;
+  const uint64_t W = (uint64_t)l.Wj * jobs;
+  if (W * l.B >= (1ull << 31)) return l;
+  l.W = (uint32_t)W;
+  l.T = l.W * l.B;
+  l.nblk = (l.T + 1023) / 1024;
+  if (l.nblk > 1024u * 64u) return l;  // the three-phase scan's limit
+  l.segs = l.T / l.L;
+  l.E = n * (uint64_t)l.Wj;
+  if (l.E >= (1ull << 32)) return l;  // entry offsets are 32-bit; pair sums < E / 2 + T < 2^32
+  // rounds: enough to bring a bucket of the mean size plus a wide margin to
+  // one point; anything left after them is folded by the tail kernel
+  const uint64_t mean = (l.E + l.T - 1) / l.T;
+  uint32_t lg = 0;
+  while ((1ull << lg) < mean) lg++;
+  l.rounds = lg + 2;
+  l.jb[0] = l.E / 2 + l.T;
+  l.jb[1] = l.jb[0] / 2 + l.T;
+  l.tasks0 = (l.jb[0] + BA_K - 1) / BA_K;
+  l.ok = true;
+  return l;
+}
+
+int sm_count() {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return sms;
+}
+
 // n: scalars (all jobs); jobs > 1: job_off (device, jobs + 1 entries) splits
 // them and every job reads bases [0, nbases); the window sums of job j are
-// windows [j W, (j + 1) W) of wout.
+// windows [j W, (j + 1) W) of wout.  bases_rp_given: the bases are already in
+// the R' form of the curve arithmetic (resident bases converted once).
 cudaError_t msm_run_impl(const fe* d_scalars, const fe* d_bases, uint64_t n, fe* d_out, cudaStream_t s,
                          int c_override, uint64_t* launches, MsmWindowsOut* wout, const uint32_t* job_off,
-                         uint32_t jobs, uint64_t nbases) {
+                         uint32_t jobs, uint64_t nbases, bool bases_rp_given) {
   uint64_t nl = 0;
   if (n == 0) {
     if (wout) {
@@ -355,113 +610,153 @@ cudaError_t msm_run_impl(const fe* d_scalars, const fe* d_bases, uint64_t n, fe*
     return cudaGetLastError();
   }
   if (jobs == 0) jobs = 1;
-  // one window size for every job: the plan of the mean job size
-  const MsmPlan p = make_msm_plan((n + jobs - 1) / jobs, c_override);
+  const MsmLayout l = msm_layout(n, jobs, c_override);
+  if (!l.ok) return cudaErrorInvalidValue;
+  const MsmPlan& p = l.p;
   if (wout) {
     if ((uint32_t)p.windows > MSM_MAX_WINDOWS || !wout->d_winsum) return cudaErrorInvalidValue;
     wout->windows = (uint32_t)p.windows;
     wout->c = (uint32_t)p.c;
   }
-  const uint32_t Wj = (uint32_t)p.windows, B = p.buckets, L = p.seg_len;
-  const uint32_t W = Wj * jobs;  // windows of all jobs
-  if ((uint64_t)W * B >= (1ull << 31)) return cudaErrorInvalidValue;
-  const uint32_t total = W * B;
-  const uint32_t nblk = (total + 1023) / 1024;
-  const uint64_t entries = n * (uint64_t)Wj;
-  if (entries >= (1ull << 32)) return cudaErrorInvalidValue;  // entry offsets are 32-bit
+  const uint32_t Wj = l.Wj, B = l.B, L = l.L, W = l.W, T = l.T, nblk = l.nblk, segs = l.segs;
+  const uint64_t entries = l.E;
   uint32_t *counts = nullptr, *offsets = nullptr, *cursor = nullptr, *bsums = nullptr, *list = nullptr;
-  uint32_t *nsub = nullptr, *sub_off = nullptr, *sub2b = nullptr, *heavy = nullptr, *heavy_count = nullptr;
-  fe *buckets = nullptr, *segres = nullptr, *winsum = nullptr, *subres = nullptr, *bases_rp = nullptr;
-  const uint32_t segs = total / L;
-  // sub-bucket size: enough sub-buckets to fill the GPU (about 2^17 threads)
-  uint32_t sub_len = SUB_MAX;
-  while (sub_len > SUB_MIN && entries / sub_len < (1ull << 17)) sub_len >>= 1;
-  // sum_b ceil(count_b / sub_len) <= entries / sub_len + total; heavy buckets have > SEQ_MAX * sub_len entries
-  const uint64_t max_sub = entries / sub_len + total + 1;
-  const uint64_t max_heavy = entries / ((uint64_t)SEQ_MAX * sub_len) + 1;
+  uint32_t *cnt = nullptr, *cprev = nullptr, *np = nullptr, *joff[2] = {nullptr, nullptr};
+  fe *fin = nullptr, *buf[2] = {nullptr, nullptr}, *pre = nullptr, *tot = nullptr, *tpre = nullptr;
+  fe *buckets = nullptr, *segres = nullptr, *winsum = nullptr, *bases_rp = nullptr;
   cudaError_t e = cudaSuccess;
   auto alloc = [&](void** ptr, size_t bytes) {
-    if (e == cudaSuccess) e = cudaMallocAsync(ptr, bytes, s);
+    if (e == cudaSuccess) e = cudaMallocAsync(ptr, bytes ? bytes : 4, s);
   };
-  alloc((void**)&counts, total * 4ull);
-  alloc((void**)&offsets, (total + 1) * 4ull);
-  alloc((void**)&cursor, total * 4ull);
-  alloc((void**)&bsums, (nblk + 1) * 4ull);
+  alloc((void**)&counts, T * 4ull);
+  alloc((void**)&offsets, (T + 1ull) * 4);
+  alloc((void**)&cursor, T * 4ull);
+  alloc((void**)&bsums, (nblk + 1ull) * 4);
   alloc((void**)&list, entries * 4ull);
-  alloc((void**)&nsub, total * 4ull);
-  alloc((void**)&sub_off, (total + 1) * 4ull);
-  alloc((void**)&sub2b, max_sub * 4ull);
-  alloc((void**)&heavy, max_heavy * 4ull);
-  alloc((void**)&heavy_count, 4ull);
-  alloc((void**)&subres, max_sub * 128ull);
-  alloc((void**)&buckets, total * 128ull);
+  alloc((void**)&cnt, T * 4ull);
+  alloc((void**)&cprev, T * 4ull);
+  alloc((void**)&np, T * 4ull);
+  alloc((void**)&joff[0], (T + 1ull) * 4);
+  alloc((void**)&joff[1], (T + 1ull) * 4);
+  alloc((void**)&fin, T * 64ull);
+  alloc((void**)&buf[0], l.jb[0] * 64);
+  if (l.rounds > 1) alloc((void**)&buf[1], l.jb[1] * 64);
+  alloc((void**)&pre, l.jb[0] * 32);
+  alloc((void**)&tot, l.tasks0 * 32);
+  alloc((void**)&tpre, l.tasks0 * 32);
+  alloc((void**)&buckets, T * 128ull);
   alloc((void**)&segres, segs * 128ull);
   if (wout)
     winsum = wout->d_winsum;  // caller's buffer, left for the host's Horner step
   else
     alloc((void**)&winsum, W * 128ull);
-  alloc((void**)&bases_rp, nbases * 64ull);
+  if (!bases_rp_given) alloc((void**)&bases_rp, nbases * 64ull);
   if (e == cudaSuccess) {
     const double nd = (double)n;
-    cudaMemsetAsync(counts, 0, total * 4ull, s);
-    cudaMemsetAsync(heavy_count, 0, 4ull, s);
+    const int sms = sm_count();
+    cudaMemsetAsync(counts, 0, T * 4ull, s);
     const unsigned g = (unsigned)((n + 255) / 256);
-    const unsigned gb = (total + 255) / 256;
-    msm_convert_bases_kernel<<<(unsigned)((nbases + 255) / 256), 256, 0, s>>>(d_bases, bases_rp, nbases);
+    const unsigned gb = (T + 255) / 256;
+    const fe* bases = d_bases;
+    if (!bases_rp_given) {
+      msm_convert_bases_kernel<<<(unsigned)((nbases + 255) / 256), 256, 0, s>>>(d_bases, bases_rp, nbases);
+      bases = bases_rp;
+      nl++;
+    }
     {
       ProfScope ps("msm_count", s, nd, nd * 32);
       msm_count_kernel<<<g, 256, 0, s>>>(d_scalars, n, (uint32_t)p.c, Wj, counts, job_off, jobs);
     }
-    scan_block_kernel<<<nblk, 1024, 0, s>>>(counts, offsets, bsums, total);
-    scan_sums_kernel<<<1, 1024, 0, s>>>(bsums, nblk, offsets + total);
-    scan_add_kernel<<<nblk, 1024, 0, s>>>(offsets, cursor, bsums, total);
+    scan_block_kernel<<<nblk, 1024, 0, s>>>(counts, offsets, bsums, T);
+    scan_sums_kernel<<<1, 1024, 0, s>>>(bsums, nblk, offsets + T);
+    scan_add_kernel<<<nblk, 1024, 0, s>>>(offsets, cursor, bsums, T);
     {
       ProfScope ps("msm_scatter", s, nd, nd * 32 + (double)entries * 4);
       msm_scatter_kernel<<<g, 256, 0, s>>>(d_scalars, n, (uint32_t)p.c, Wj, cursor, list, job_off, jobs);
     }
-    msm_nsub_kernel<<<gb, 256, 0, s>>>(counts, nsub, total, sub_len);
-    scan_block_kernel<<<nblk, 1024, 0, s>>>(nsub, sub_off, bsums, total);
-    scan_sums_kernel<<<1, 1024, 0, s>>>(bsums, nblk, sub_off + total);
-    scan_add_kernel<<<nblk, 1024, 0, s>>>(sub_off, cursor, bsums, total);
-    msm_submap_kernel<<<gb, 256, 0, s>>>(nsub, sub_off, sub2b, total);
+    nl += 5;
     {
-      // convention: 6 Fq products per point-window (batch-affine cost)
-      ProfScope ps("msm_bucket", s, (double)entries * 6, (double)entries * (64 + 4) + max_sub * 128.0);
-      msm_subbucket_kernel<<<(unsigned)((max_sub + 255) / 256), 256, 0, s>>>(list, offsets, counts, sub_off, sub2b,
-                                                                              sub_off + total, bases_rp, subres, sub_len);
+      // convention: 6 Fq products per point-window (the batch-affine cost);
+      // algorithmic bytes: each entry's index and signed base read once
+      ProfScope ps("msm_bucket", s, (double)entries * 6, (double)entries * 68);
+      ba_setup_kernel<<<gb, 256, 0, s>>>(counts, offsets, list, bases, cnt, fin, T);
+      nl++;
+      uint64_t jb = l.jb[0];
+      for (uint32_t r = 0; r < l.rounds; r++) {
+        const bool first = r == 0;
+        uint32_t* jo = joff[r & 1];
+        const uint32_t* in_off = first ? offsets : joff[(r + 1) & 1];
+        const fe* src = first ? bases : buf[(r + 1) & 1];
+        fe* dst = buf[r & 1];
+        ba_jobs_kernel<<<gb, 256, 0, s>>>(cnt, cprev, np, T);
+        scan_block_kernel<<<nblk, 1024, 0, s>>>(np, jo, bsums, T);
+        scan_sums_kernel<<<1, 1024, 0, s>>>(bsums, nblk, jo + T);
+        scan_add_kernel<<<nblk, 1024, 0, s>>>(jo, cursor, bsums, T);
+        const uint64_t tasks = (jb + BA_K - 1) / BA_K, groups = (tasks + BA_G - 1) / BA_G;
+        const unsigned gt = (unsigned)std::min<uint64_t>((tasks + 255) / 256, (uint64_t)sms * 6);
+        const unsigned gi = (unsigned)std::min<uint64_t>((groups + 127) / 128, (uint64_t)sms * 8);
+        if (first)
+          ba_prefix_kernel<true><<<gt, 256, 0, s>>>(src, list, in_off, cprev, jo, np, T, pre, tot);
+        else
+          ba_prefix_kernel<false><<<gt, 256, 0, s>>>(src, list, in_off, cprev, jo, np, T, pre, tot);
+        ba_invert_kernel<<<gi, 128, 0, s>>>(tot, tpre, jo, T);
+        if (first)
+          ba_apply_kernel<true><<<gt, 256, 0, s>>>(src, list, in_off, cprev, jo, np, T, pre, tot, dst, fin, cnt);
+        else
+          ba_apply_kernel<false><<<gt, 256, 0, s>>>(src, list, in_off, cprev, jo, np, T, pre, tot, dst, fin, cnt);
+        nl += 7;
+        jb = jb / 2 + T;
+      }
+      const uint32_t last = (l.rounds - 1) & 1;
+      ba_tail_kernel<<<gb, 256, 0, s>>>(cnt, joff[last], buf[last], fin, buckets, T);
+      nl++;
     }
     {
-      ProfScope ps("msm_bucket_final", s, (double)total * 14, total * 256.0);
-      msm_bucket_final_kernel<<<gb, 256, 0, s>>>(nsub, sub_off, subres, buckets, heavy, heavy_count, total);
-      msm_heavy_kernel<<<(unsigned)max_heavy, 256, 0, s>>>(nsub, sub_off, subres, buckets, heavy, heavy_count);
-    }
-    {
-      ProfScope ps("msm_segment", s, (double)total * 2 * 14, total * 128.0);
+      ProfScope ps("msm_segment", s, (double)T * 2 * 14, T * 128.0);
       msm_segment_kernel<<<(segs + 127) / 128, 128, 0, s>>>(buckets, segres, B, L, segs);
     }
     msm_window_kernel<<<W, 256, 0, s>>>(segres, winsum, B / L);
-    if (!wout) msm_combine_kernel<<<1, 32, 0, s>>>(winsum, W, (uint32_t)p.c, d_out);
-    nl = wout ? 16 : 17;
+    nl += 2;
+    if (!wout) {
+      msm_combine_kernel<<<1, 32, 0, s>>>(winsum, W, (uint32_t)p.c, d_out);
+      nl++;
+    }
     e = cudaGetLastError();
   }
-  for (void* ptr : {(void*)counts, (void*)offsets, (void*)cursor, (void*)bsums, (void*)list, (void*)nsub,
-                    (void*)sub_off, (void*)sub2b, (void*)heavy, (void*)heavy_count, (void*)subres, (void*)buckets,
-                    (void*)segres, (void*)(wout ? nullptr : winsum), (void*)bases_rp})
+  for (void* ptr : {(void*)counts, (void*)offsets, (void*)cursor, (void*)bsums, (void*)list, (void*)cnt,
+                    (void*)cprev, (void*)np, (void*)joff[0], (void*)joff[1], (void*)fin, (void*)buf[0],
+                    (void*)buf[1], (void*)pre, (void*)tot, (void*)tpre, (void*)buckets, (void*)segres,
+                    (void*)(wout ? nullptr : winsum), (void*)bases_rp})
     if (ptr) cudaFreeAsync(ptr, s);
   if (launches) *launches = nl;
   return e;
 }
 }  // namespace
 
+uint64_t msm_scratch_bytes(uint64_t n_total, uint32_t jobs, uint64_t nbases, bool bases_rp_given, bool own_winsum,
+                           int device) {
+  if (n_total == 0) return 256;
+  const MsmLayout l = msm_layout(n_total, jobs, 0, device);
+  if (!l.ok) return ~0ull >> 2;
+  return l.bytes(own_winsum, bases_rp_given ? 0 : nbases);
+}
+
+cudaError_t msm_convert_bases(const fe* d_in, fe* d_out, uint64_t n, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  msm_convert_bases_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(d_in, d_out, n);
+  return cudaGetLastError();
+}
+
 cudaError_t msm_run(const fe* d_scalars, const fe* d_bases, uint64_t n, fe* d_out, cudaStream_t s, int c_override,
-                    uint64_t* launches, MsmWindowsOut* wout) {
-  return msm_run_impl(d_scalars, d_bases, n, d_out, s, c_override, launches, wout, nullptr, 1, n);
+                    uint64_t* launches, MsmWindowsOut* wout, bool bases_rp) {
+  return msm_run_impl(d_scalars, d_bases, n, d_out, s, c_override, launches, wout, nullptr, 1, n, bases_rp);
 }
 
 cudaError_t msm_run_multi(const fe* d_scalars, const fe* d_bases, const uint32_t* d_job_off, uint32_t jobs,
-                          uint64_t n_total, uint64_t max_n, cudaStream_t s, uint64_t* launches, MsmWindowsOut* wout) {
+                          uint64_t n_total, uint64_t max_n, cudaStream_t s, uint64_t* launches, MsmWindowsOut* wout,
+                          bool bases_rp) {
   if (!wout || !wout->d_winsum || jobs == 0 || !d_job_off || n_total >= (1ull << 32)) return cudaErrorInvalidValue;
-  return msm_run_impl(d_scalars, d_bases, n_total, nullptr, s, 0, launches, wout, d_job_off, jobs, max_n);
+  return msm_run_impl(d_scalars, d_bases, n_total, nullptr, s, 0, launches, wout, d_job_off, jobs, max_n, bases_rp);
 }
 
 }  // namespace zk

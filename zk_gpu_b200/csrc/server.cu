@@ -33,13 +33,11 @@ namespace zk {
 namespace {
 using clk = std::chrono::steady_clock;
 
-uint64_t msm_scratch_bytes(uint64_t n) {
-  if (n == 0) return 256;
-  const MsmPlan p = make_msm_plan(n);
-  const uint64_t total = (uint64_t)p.windows * p.buckets;
-  const uint64_t entries = n * p.windows;
-  const uint64_t max_sub = entries / 16 + total + 1;  // smallest sub-bucket size msm_run uses
-  return total * 4 * 6 + entries * 4 + max_sub * (4 + 128) + total * 128 * 2 + 4096;
+// Device memory one MSM job of n points holds in flight when it runs alone:
+// its scalars, its window sums and the pass's scratch (resident bases are
+// already in the curve arithmetic's form, so nothing is converted).
+uint64_t msm_job_bytes(uint64_t n, int device) {
+  return n * 32 + MSM_MAX_WINDOWS * 128ull + msm_scratch_bytes(n, 1, n, true, false, device);
 }
 
 host::Fr fr_of(const uint64_t v[4]) {
@@ -125,6 +123,10 @@ class Server {
     b.n = n;
     ZK_TRY("cudaMalloc(bases)", cudaMalloc((void**)&b.d, std::max<uint64_t>(bytes, 64)));
     ZK_TRY("bases H2D", cudaMemcpy(b.d, xy, bytes, cudaMemcpyHostToDevice));
+    // resident bases are kept in the curve arithmetic's R' form: converted
+    // once here instead of on every MSM over them
+    ZK_TRY("bases convert", msm_convert_bases(b.d, b.d, n, s_msm_[0]));
+    ZK_TRY("bases convert sync", cudaStreamSynchronize(s_msm_[0]));
     std::lock_guard<std::mutex> lk(mu_);
     bases_.push_back(b);
     *id = (uint32_t)bases_.size() - 1;
@@ -134,7 +136,7 @@ class Server {
   int submit(const zkgpu_job* job, uint64_t* ticket) {
     auto rec = std::make_unique<JobRec>();
     rec->job = *job;
-    rec->bytes = zkgpu_job_footprint(job);
+    rec->bytes = job->kind == ZKGPU_KIND_MSM ? msm_job_bytes(job->n, device_) : zkgpu_job_footprint(job);
     rec->t_submit = clk::now();
     std::lock_guard<std::mutex> lk(mu_);
     if (stop_) return ZKGPU_EBUSY;
@@ -269,13 +271,28 @@ class Server {
     std::map<uint32_t, std::vector<JobRec*>> msm_groups;
     for (JobRec* r : w.jobs)
       if (r->job.kind == ZKGPU_KIND_MSM) msm_groups[r->job.bases_id].push_back(r);
-    // merged passes keep their 32-bit entry offsets: at most 2^25 scalars
-    auto merged = [&](uint32_t bases_id) {
-      const std::vector<JobRec*>& grp = msm_groups[bases_id];
-      uint64_t tot = 0;
-      for (const JobRec* r : grp) tot += r->job.n;
-      return grp.size() >= 2 && tot <= (1ull << 25);
-    };
+    // A group merges when its jobs fit one pass: 32-bit entry offsets (at
+    // most 2^25 scalars) and the merged pass's device memory (one window
+    // size from the mean job size, so a skewed group can need more than its
+    // jobs alone) within the bytes the jobs were admitted with.
+    std::map<uint32_t, bool> merge_ok;
+    for (auto& g : msm_groups) {
+      const std::vector<JobRec*>& grp = g.second;
+      uint64_t tot = 0, max_n = 0, admitted = 0;
+      for (const JobRec* r : grp) {
+        tot += r->job.n;
+        max_n = std::max<uint64_t>(max_n, r->job.n);
+        admitted += r->bytes;
+      }
+      bool ok_merge = grp.size() >= 2 && tot <= (1ull << 25);
+      if (ok_merge) {
+        const uint64_t need = tot * 32 + grp.size() * (MSM_MAX_WINDOWS * 128ull + 4) +
+                              msm_scratch_bytes(tot, (uint32_t)grp.size(), max_n, true, false, device_);
+        ok_merge = need <= admitted;
+      }
+      merge_ok[g.first] = ok_merge;
+    }
+    auto merged = [&](uint32_t bases_id) { return merge_ok[bases_id]; };
     for (auto& g : msm_groups) {
       std::vector<JobRec*>& grp = g.second;
       if (!merged(g.first)) continue;
@@ -304,7 +321,7 @@ class Server {
         uint64_t nl = 0;
         MsmWindowsOut wo;
         wo.d_winsum = dwin;
-        if (ok(msm_run_multi(ds, bs.d, doff, (uint32_t)grp.size(), n_total, max_n, w.s_msm, &nl, &wo))) {
+        if (ok(msm_run_multi(ds, bs.d, doff, (uint32_t)grp.size(), n_total, max_n, w.s_msm, &nl, &wo, true))) {
           merged_passes_++;
           merged_jobs_ += grp.size();
           for (size_t k = 0; k < grp.size(); k++) {
@@ -336,7 +353,7 @@ class Server {
           uint64_t nl = 0;
           MsmWindowsOut wo;
           wo.d_winsum = dwin;
-          if (ok(msm_run(ds, bs.d, j.n, nullptr, w.s_msm, 0, &nl, &wo))) {
+          if (ok(msm_run(ds, bs.d, j.n, nullptr, w.s_msm, 0, &nl, &wo, true))) {
             r->msm_out = next_msm_slot;
             next_msm_slot += kMsmSlotWords;
             r->msm_out[0] = wo.windows;
@@ -539,8 +556,11 @@ extern "C" uint64_t zkgpu_job_footprint(const zkgpu_job* j) {
       return 2 * ((uint64_t)1 << j->log_n) * 32 + 4096;
     case ZKGPU_KIND_LDE:
       return 2 * ((uint64_t)1 << j->log_ext) * 32 + 4096;
-    case ZKGPU_KIND_MSM:
-      return j->n * 32 + zk::msm_scratch_bytes(j->n);
+    case ZKGPU_KIND_MSM: {
+      int dev = 0;
+      cudaGetDevice(&dev);
+      return zk::msm_job_bytes(j->n, dev);
+    }
     default:
       return 0;
   }
