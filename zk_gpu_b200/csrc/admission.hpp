@@ -34,6 +34,14 @@ class AdmissionQueue {
     return true;
   }
   uint64_t reserved() const { return reserved_; }
+  // take `bytes` more for work already admitted (e.g. a merged pass that
+  // needs more than its jobs' footprints) if they are free now; give them
+  // back with release()
+  bool take(uint64_t bytes) {
+    if (used_ > budget_ || bytes > budget_ - used_) return false;
+    used_ += bytes;
+    return true;
+  }
   // admit jobs in FIFO order while the head fits; returns admitted tickets
   std::vector<uint64_t> admit(size_t max_jobs = SIZE_MAX) {
     std::vector<uint64_t> out;

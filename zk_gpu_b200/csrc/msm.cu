@@ -422,27 +422,91 @@ __global__ void __launch_bounds__(256) ba_apply_kernel(const fe* src, const uint
   }
 }
 
-// tail: every bucket to XYZZ; buckets still holding more than one point
-// (skewed inputs past the last round) are folded with mixed additions
-__global__ void ba_tail_kernel(const uint32_t* cnt, const uint32_t* in_off, const fe* src, const fe* fin,
-                               fe* buckets, uint32_t T) {
+// Tail: what the rounds left (a few points per bucket, or many in a skewed
+// bucket such as the one small scalars carry into) is folded with XYZZ mixed
+// additions in chunks of BA_TS points, one thread per chunk; a bucket's
+// chunk sums are then added by one thread, or block-wide when there are many.
+constexpr uint32_t BA_TS = 16;    // points per tail chunk
+constexpr uint32_t BA_TSEQ = 16;  // chunk sums a bucket adds in one thread
+
+__global__ void ba_chunks_kernel(const uint32_t* cnt, uint32_t* nch, uint32_t T) {
   const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= T) return;
   const uint32_t c = cnt[b];
-  xyzz_t acc;
-  xyzz_set_inf(acc);
-  aff_t p;
-  if (c <= 1) {
-    ld_aff(p, fin + 2 * (uint64_t)b);
-    xyzz_from_aff(acc, p);  // (0, 0) -> identity
-  } else {
-    const uint32_t o = in_off[b];
-    for (uint32_t i = 0; i < c; i++) {
-      ld_aff(p, src + 2 * (uint64_t)(o + i));
-      xyzz_madd(acc, p);
+  nch[b] = c <= 1 ? 1u : (c + BA_TS - 1) / BA_TS;
+}
+
+__global__ void __launch_bounds__(256) ba_fold_kernel(const uint32_t* cnt, const uint32_t* in_off, const fe* src,
+                                                      const fe* fin, const uint32_t* coff, const uint32_t* nch,
+                                                      uint32_t T, fe* chunk_res) {
+  const uint32_t C = coff[T];
+  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < C; u += gridDim.x * blockDim.x) {
+    const uint32_t b = ba_bucket_of(coff, T, u);
+    const uint32_t k = u - coff[b], c = cnt[b];
+    xyzz_t acc;
+    xyzz_set_inf(acc);
+    aff_t p;
+    if (c <= 1) {
+      ld_aff(p, fin + 2 * (uint64_t)b);
+      xyzz_from_aff(acc, p);  // (0, 0) -> identity
+    } else {
+      const uint32_t o = in_off[b], i1 = min(c, (k + 1) * BA_TS);
+      for (uint32_t i = k * BA_TS; i < i1; i++) {
+        ld_aff(p, src + 2 * (uint64_t)(o + i));
+        xyzz_madd(acc, p);
+      }
     }
+    st_xyzz(chunk_res + 4 * (uint64_t)u, acc);
+  }
+}
+
+__global__ void ba_bucket_sum_kernel(const uint32_t* coff, const uint32_t* nch, const fe* chunk_res, fe* buckets,
+                                     uint32_t* heavy, uint32_t* heavy_count, uint32_t T) {
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= T) return;
+  const uint32_t k = nch[b], o = coff[b];
+  if (k > BA_TSEQ) {
+    heavy[atomicAdd(heavy_count, 1u)] = b;
+    return;
+  }
+  xyzz_t acc, t;
+  ld_xyzz(acc, chunk_res + 4 * (uint64_t)o);
+  for (uint32_t j = 1; j < k; j++) {
+    ld_xyzz(t, chunk_res + 4 * (uint64_t)(o + j));
+    xyzz_add(acc, t);
   }
   st_xyzz(buckets + 4 * (uint64_t)b, acc);
+}
+
+// One block per queued heavy bucket: strided partial sums, then a tree.
+__global__ void __launch_bounds__(256) ba_heavy_kernel(const uint32_t* coff, const uint32_t* nch, const fe* chunk_res,
+                                                       fe* buckets, const uint32_t* heavy,
+                                                       const uint32_t* heavy_count) {
+  __shared__ fe sh[256 * 4];
+  if (blockIdx.x >= *heavy_count) return;
+  const uint32_t b = heavy[blockIdx.x];
+  const uint32_t k = nch[b], o = coff[b];
+  xyzz_t acc, t;
+  xyzz_set_inf(acc);
+  for (uint32_t j = threadIdx.x; j < k; j += blockDim.x) {
+    ld_xyzz(t, chunk_res + 4 * (uint64_t)(o + j));
+    xyzz_add(acc, t);
+  }
+  st_xyzz(sh + 4 * threadIdx.x, acc);
+  __syncthreads();
+  for (uint32_t half = blockDim.x / 2; half > 0; half >>= 1) {
+    if (threadIdx.x < half) {
+      ld_xyzz(acc, sh + 4 * threadIdx.x);
+      ld_xyzz(t, sh + 4 * (threadIdx.x + half));
+      xyzz_add(acc, t);
+      st_xyzz(sh + 4 * threadIdx.x, acc);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    ld_xyzz(acc, sh);
+    st_xyzz(buckets + 4 * (uint64_t)b, acc);
+  }
 }
 
 // Per (window, segment): running sums over the segment's buckets, top down,
@@ -541,6 +605,7 @@ struct MsmLayout {
   uint64_t E = 0;                // entries (point-window pairs), upper bound
   uint64_t jb[2] = {0, 0};       // pair sums of rounds 0 and 1, upper bounds
   uint64_t tasks0 = 0;
+  uint64_t chunks = 0;           // tail chunks, upper bound
   bool ok = false;
   uint64_t bytes(bool own_winsum, uint64_t nbases_convert) const {
     const uint64_t T1 = T + 1ull;
@@ -549,6 +614,7 @@ struct MsmLayout {
     b += T * 4ull * 3 + T1 * 4 * 2 + T * 64ull;                   // cnt, cprev, np, joff x2, fin
     b += jb[0] * 64 + (rounds > 1 ? jb[1] * 64 : 0) + jb[0] * 32;  // round buffers, prefixes
     b += tasks0 * 32 * 2;                                         // task products, their prefixes
+    b += T * 4ull * 2 + chunks * 128 + 4;                         // tail: chunk counts, heavy list, chunk sums
     b += T * 128ull + segs * 128ull + (own_winsum ? W * 128ull : 0);
     b += nbases_convert * 64;
     return b + 24 * 256;  // pool granularity per allocation
@@ -576,10 +642,15 @@ MsmLayout msm_layout(uint64_t n, uint32_t jobs, int c_override, int device = -1)
   const uint64_t mean = (l.E + l.T - 1) / l.T;
   uint32_t lg = 0;
   while ((1ull << lg) < mean) lg++;
-  l.rounds = lg + 2;
+  // batch-affine rounds while buckets hold more than about four points;
+  // later levels cost more in per-round latency than they save
+  l.rounds = lg > 3 ? lg - 2 : 1;
   l.jb[0] = l.E / 2 + l.T;
   l.jb[1] = l.jb[0] / 2 + l.T;
   l.tasks0 = (l.jb[0] + BA_K - 1) / BA_K;
+  uint64_t jlast = l.jb[0];
+  for (uint32_t r = 1; r < l.rounds; r++) jlast = jlast / 2 + l.T;
+  l.chunks = l.T + jlast / BA_TS + 1;  // bound on sum_b max(1, ceil(cnt_b / BA_TS))
   l.ok = true;
   return l;
 }
@@ -623,7 +694,8 @@ cudaError_t msm_run_impl(const fe* d_scalars, const fe* d_bases, uint64_t n, fe*
   uint32_t *counts = nullptr, *offsets = nullptr, *cursor = nullptr, *bsums = nullptr, *list = nullptr;
   uint32_t *cnt = nullptr, *cprev = nullptr, *np = nullptr, *joff[2] = {nullptr, nullptr};
   fe *fin = nullptr, *buf[2] = {nullptr, nullptr}, *pre = nullptr, *tot = nullptr, *tpre = nullptr;
-  fe *buckets = nullptr, *segres = nullptr, *winsum = nullptr, *bases_rp = nullptr;
+  fe *buckets = nullptr, *segres = nullptr, *winsum = nullptr, *bases_rp = nullptr, *chunk_res = nullptr;
+  uint32_t *nch = nullptr, *heavy = nullptr, *heavy_count = nullptr;
   cudaError_t e = cudaSuccess;
   auto alloc = [&](void** ptr, size_t bytes) {
     if (e == cudaSuccess) e = cudaMallocAsync(ptr, bytes ? bytes : 4, s);
@@ -644,6 +716,10 @@ cudaError_t msm_run_impl(const fe* d_scalars, const fe* d_bases, uint64_t n, fe*
   alloc((void**)&pre, l.jb[0] * 32);
   alloc((void**)&tot, l.tasks0 * 32);
   alloc((void**)&tpre, l.tasks0 * 32);
+  alloc((void**)&nch, T * 4ull);
+  alloc((void**)&heavy, T * 4ull);
+  alloc((void**)&heavy_count, 4);
+  alloc((void**)&chunk_res, l.chunks * 128);
   alloc((void**)&buckets, T * 128ull);
   alloc((void**)&segres, segs * 128ull);
   if (wout)
@@ -707,9 +783,20 @@ cudaError_t msm_run_impl(const fe* d_scalars, const fe* d_bases, uint64_t n, fe*
         nl += 7;
         jb = jb / 2 + T;
       }
+      // tail: chunk counts -> scan (offsets in joff of the unused parity) -> folds -> bucket sums
       const uint32_t last = (l.rounds - 1) & 1;
-      ba_tail_kernel<<<gb, 256, 0, s>>>(cnt, joff[last], buf[last], fin, buckets, T);
-      nl++;
+      uint32_t* coff = joff[last ^ 1];
+      ba_chunks_kernel<<<gb, 256, 0, s>>>(cnt, nch, T);
+      scan_block_kernel<<<nblk, 1024, 0, s>>>(nch, coff, bsums, T);
+      scan_sums_kernel<<<1, 1024, 0, s>>>(bsums, nblk, coff + T);
+      scan_add_kernel<<<nblk, 1024, 0, s>>>(coff, cursor, bsums, T);
+      cudaMemsetAsync(heavy_count, 0, 4, s);
+      const unsigned gf = (unsigned)std::min<uint64_t>((l.chunks + 255) / 256, (uint64_t)sms * 8);
+      ba_fold_kernel<<<gf, 256, 0, s>>>(cnt, joff[last], buf[last], fin, coff, nch, T, chunk_res);
+      ba_bucket_sum_kernel<<<gb, 256, 0, s>>>(coff, nch, chunk_res, buckets, heavy, heavy_count, T);
+      const uint64_t max_heavy = std::min<uint64_t>(T, l.chunks / (BA_TSEQ + 1) + 1);
+      ba_heavy_kernel<<<(unsigned)max_heavy, 256, 0, s>>>(coff, nch, chunk_res, buckets, heavy, heavy_count);
+      nl += 8;
     }
     {
       ProfScope ps("msm_segment", s, (double)T * 2 * 14, T * 128.0);
@@ -726,6 +813,7 @@ cudaError_t msm_run_impl(const fe* d_scalars, const fe* d_bases, uint64_t n, fe*
   for (void* ptr : {(void*)counts, (void*)offsets, (void*)cursor, (void*)bsums, (void*)list, (void*)cnt,
                     (void*)cprev, (void*)np, (void*)joff[0], (void*)joff[1], (void*)fin, (void*)buf[0],
                     (void*)buf[1], (void*)pre, (void*)tot, (void*)tpre, (void*)buckets, (void*)segres,
+                    (void*)nch, (void*)heavy, (void*)heavy_count, (void*)chunk_res,
                     (void*)(wout ? nullptr : winsum), (void*)bases_rp})
     if (ptr) cudaFreeAsync(ptr, s);
   if (launches) *launches = nl;

@@ -61,6 +61,7 @@ struct Wave {
   cudaEvent_t ev_ntt = nullptr, ev_msm = nullptr;
   std::vector<BatchPass> passes;  // host copy kept alive for the async upload
   uint64_t* mailbox = nullptr;    // pinned: [0] batch error flag, then kMsmSlotWords per MSM job
+  uint64_t extra_bytes = 0;       // budget taken beyond the jobs' footprints (merged MSM passes)
   int status = ZKGPU_OK;
 };
 
@@ -274,7 +275,8 @@ class Server {
     // A group merges when its jobs fit one pass: 32-bit entry offsets (at
     // most 2^25 scalars) and the merged pass's device memory (one window
     // size from the mean job size, so a skewed group can need more than its
-    // jobs alone) within the bytes the jobs were admitted with.
+    // jobs alone) within the bytes the jobs were admitted with, plus what
+    // the budget has free now (taken until the wave retires).
     std::map<uint32_t, bool> merge_ok;
     for (auto& g : msm_groups) {
       const std::vector<JobRec*>& grp = g.second;
@@ -288,7 +290,14 @@ class Server {
       if (ok_merge) {
         const uint64_t need = tot * 32 + grp.size() * (MSM_MAX_WINDOWS * 128ull + 4) +
                               msm_scratch_bytes(tot, (uint32_t)grp.size(), max_n, true, false, device_);
-        ok_merge = need <= admitted;
+        if (need > admitted) {  // borrow the difference from the free budget until the wave retires
+          std::lock_guard<std::mutex> lk(mu_);
+          ok_merge = adm_.take(need - admitted);
+          if (ok_merge) {
+            w.extra_bytes += need - admitted;
+            peak_ = std::max(peak_, adm_.used() + adm_.reserved());
+          }
+        }
       }
       merge_ok[g.first] = ok_merge;
     }
@@ -518,6 +527,7 @@ class Server {
           else
             failed_++;
         }
+        adm_.release(w->extra_bytes);
         inflight_jobs_ -= w->jobs.size();
         waves_inflight_--;
         retired_gen_++;
