@@ -232,6 +232,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     d_vals = torch.from_numpy(vals_np.view(np.int64)).to(f"cuda:{dev}")
     d_ext = torch.empty((N, 4), dtype=torch.int64, device=f"cuda:{dev}")
     stream = torch.cuda.Stream(device=dev)
+    torch.cuda.synchronize()
 
     imad_ps, modmul_ps = zk.int_peak(dev)
 
@@ -290,6 +291,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
 
     # ---- forward NTT 2^24 (sub-metric) ----
     d_a = d_vals.clone()
+    torch.cuda.synchronize()
     for _ in range(3):
         zk.ntt_dev(d_a, LOG_N, c["omega"], stream=stream)
     stream.synchronize()
@@ -308,6 +310,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     d_sc = torch.from_numpy(sc.view(np.int64)).to(f"cuda:{dev}")
     d_bs = gen_bases(zk, torch, n_msm, 4141 + rank, dev)
     d_out = torch.zeros(12, dtype=torch.int64, device=f"cuda:{dev}")
+    torch.cuda.synchronize()
     zk.msm_dev(d_sc, d_bs, d_out, stream=stream)
     stream.synchronize()
     msm_steps = max(3, min(args.steps, 10))
@@ -489,6 +492,7 @@ def bench_batched(zk, torch, dev: int, stream, steps: int, njobs: int = 512, see
         jobs.append(j)
     elems = sum(1 << k for k in sizes)
     orig = [j["tensor"].clone() for j in jobs]
+    torch.cuda.synchronize()  # inputs are made on torch's stream; the runs below use `stream`
     batch = zk.NttBatch(jobs, device=dev)
     for _ in range(2):
         batch.run(stream)
@@ -523,16 +527,20 @@ def bench_batched(zk, torch, dev: int, stream, steps: int, njobs: int = 512, see
     single_ms = e0.elapsed_time(e1) / runs
     # verification: every batched output against the one-call-per-job output
     # of the same job on the same (restored) seeded input, compared on the GPU
+    torch.cuda.synchronize()
     for j, o in zip(jobs, orig):
         j["tensor"].copy_(o)
+    torch.cuda.synchronize()
     batch.run(stream)
     stream.synchronize()
     batch.check()
     got = [j["tensor"].clone() for j in jobs]
     for j, o in zip(jobs, orig):
         j["tensor"].copy_(o)
+    torch.cuda.synchronize()
     one_call_per_job()
     stream.synchronize()
+    torch.cuda.synchronize()
     verified = sum(bool(torch.equal(g, j["tensor"])) for g, j in zip(got, jobs))
     del got
     info = batch.info()
@@ -961,6 +969,7 @@ def run_case(args):
 
         def step():
             zk.msm_dev(s, b, out, stream=stream)
+    torch.cuda.synchronize()  # inputs were made on torch's stream
     step()
     stream.synchronize()
     e0.record(stream)
