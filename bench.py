@@ -737,18 +737,19 @@ def bench_serving(zk, torch, dev: int, njobs: int = 1000, rate: float = 2000.0, 
     lam1 = 0.8 * one_cap
     lat_p1, span_p1 = run_plain(lam1)
     p99_budget = pct(lat_p1, 99)
+    # a rate is sustained at equal p99 when the serving loop's p99 stays within
+    # the one-call arm's (a backlog would grow the p99 without bound)
     sweep = []
     best = None
-    for mult in (1.0, 2.0, 3.0, 3.5, 4.0, 5.0, 6.0, 8.0):
+    for mult in (1.0, 2.0, 2.5, 3.0, 3.5, 4.0, 5.0, 6.0, 8.0):
         lam = lam1 * mult
         lat_b, span_b = run_server(lam)
-        ach = n / span_b
-        rec = {"offered_jobs_s": round(lam, 1), "achieved_jobs_s": round(ach, 1),
+        rec = {"offered_jobs_s": round(lam, 1), "achieved_jobs_s": round(n / span_b, 1),
                "p50_ms": round(pct(lat_b, 50) * 1e3, 2), "p99_ms": round(pct(lat_b, 99) * 1e3, 2)}
         sweep.append(rec)
-        if pct(lat_b, 99) <= p99_budget and ach >= 0.95 * lam:
+        if pct(lat_b, 99) <= p99_budget:
             best = rec
-        elif best is not None:
+        else:
             break
     # ---- verification: every job, batched (in waves, own buffers) vs alone ----
     verified, checked, chunk = 0, 0, []
@@ -825,12 +826,13 @@ def bench_serving(zk, torch, dev: int, njobs: int = 1000, rate: float = 2000.0, 
                  "batched_closed_loop_d2h_gbs": round(d2h / span_sc / 1e9, 2),
                  "batched_closed_loop_h2d_gbs": round(h2d / span_sc / 1e9, 2),
                  "one_call_closed_loop_d2h_gbs": round(d2h / span_pc / 1e9, 2)})
-    eq = None
-    if best is not None:
-        eq = {"p99_budget_ms": round(p99_budget * 1e3, 2),
-              "one_call": {"offered_jobs_s": round(lam1, 1), "achieved_jobs_s": round(n / span_p1, 1),
-                           "p99_ms": round(p99_budget * 1e3, 2)},
-              "batched": best, "jobs_s_ratio": round(best["achieved_jobs_s"] / (n / span_p1), 3)}
+    eq = {"p99_budget_ms": round(p99_budget * 1e3, 2),
+          "one_call": {"offered_jobs_s": round(lam1, 1), "achieved_jobs_s": round(n / span_p1, 1),
+                       "p50_ms": round(pct(lat_p1, 50) * 1e3, 2), "p99_ms": round(p99_budget * 1e3, 2)},
+          "batched": best,
+          "jobs_s_ratio": round(best["offered_jobs_s"] / lam1, 3) if best else None,
+          "rule": "same Poisson trace; the serving loop's largest offered rate with p99 <= the one-call arm's "
+                  "p99 at 80% of its saturation throughput; ratio of offered rates"}
     return {
         "jobs": n, "offered_rate_jobs_s": rate,
         "mix": "35% NTT 2^12-2^22, 35% coset LDE x4 2^12-2^22, 30% MSM 2^14-2^20 (resident 2^20 bases)",

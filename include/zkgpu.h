@@ -292,6 +292,14 @@ int zkgpu_field_op(int device, int op, int fid, const uint64_t *a, const uint64_
  * ZKGPU_ETIMEOUT (omega12: a root of order 2^12).  No counterpart in the
  * reference, whose scheduler waits without limit (src/gpulock.rs:191-194). */
 int zkgpu_selftest_wait_timeout(int device, const uint64_t omega12[4], uint32_t spin_us);
+/* Give back the device memory the library keeps cached on `device`: the
+ * NTT / coset table caches (capped at ZKGPU_TABLE_CACHE_MB per device,
+ * default 8192, least recently used first; a serving loop counts them against
+ * its HBM budget) and the unused blocks of the library's own memory pool.
+ * Tables still read by live batches or in-flight work stay allocated until
+ * that work lets go of them.  No counterpart in the reference, which
+ * allocates and frees everything per call (cuda/fft.cu:282-328). */
+int zkgpu_release_cached(int device);
 /* message of the last ZKGPU_ECUDA on this thread ("" if none) */
 const char *zkgpu_last_error(void);
 /* kernel launches issued by this thread since the last reset */

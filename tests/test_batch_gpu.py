@@ -78,3 +78,26 @@ def test_batch_matches_single_calls(zk, oracle):
     batch.check()
     assert torch.equal(alone, mixed)
     batch.close()
+
+
+def test_release_cached_keeps_live_batches_correct(zk, oracle):
+    """zkgpu_release_cached drops the device's cached tables and pooled
+    memory; a batch built before it still holds its own tables, and the next
+    plain call rebuilds what it needs — all results stay bit-exact."""
+    torch = pytest.importorskip("torch")
+    k = 14
+    a = oracle.rand_fr(1 << k, 91)
+    w = oracle.omega(k)
+    t = torch.from_numpy(a.view(np.int64)).cuda()
+    batch = zk.NttBatch([{"tensor": t, "log_n": k, "omega": w}])
+    zk.release_cached(0)
+    batch.run()
+    torch.cuda.synchronize()
+    batch.check()
+    assert np.array_equal(t.cpu().numpy().view(np.uint64), oracle.best_fft(a, w, k))
+    batch.close()
+    zk.release_cached(0)
+    t2 = torch.from_numpy(a.view(np.int64)).cuda()
+    zk.ntt_dev(t2, k, w)
+    torch.cuda.synchronize()
+    assert np.array_equal(t2.cpu().numpy().view(np.uint64), oracle.best_fft(a, w, k))

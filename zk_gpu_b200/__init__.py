@@ -104,6 +104,7 @@ EXPORTS = {
     "zkgpu_server_stats_get": (_i32, [P, P]),
     "zkgpu_server_destroy": (None, [P]),
     "zkgpu_field_op": (_i32, [_i32, _i32, _i32, P, P, P, _u64]),
+    "zkgpu_release_cached": (_i32, [_i32]),
     "zkgpu_last_error": (ctypes.c_char_p, []),
     "zkgpu_launch_count": (_u64, [_i32]),
     "zkgpu_version": (ctypes.c_char_p, []),
@@ -236,6 +237,11 @@ def field_op(op: str, a: np.ndarray, b: np.ndarray, field: str = "fr", device: i
     _check(lib().zkgpu_field_op(device, {"mul": 0, "add": 1, "sub": 2}[op], {"fr": 0, "fq": 1}[field],
                                 a.ctypes.data, b.ctypes.data, out.ctypes.data, a.shape[0]), "field_op")
     return out
+
+
+def release_cached(device: int = 0):
+    """Free the library's cached tables and pooled memory on `device`."""
+    _check(lib().zkgpu_release_cached(device), "release_cached")
 
 
 def launch_count(reset: bool = False) -> int:

@@ -34,18 +34,23 @@ class AdmissionQueue {
     return true;
   }
   uint64_t reserved() const { return reserved_; }
+  // device memory held outside the jobs (the library's table caches), set
+  // before each admission round; it counts against the same budget
+  void set_external(uint64_t bytes) { external_ = bytes; }
+  uint64_t external() const { return external_; }
   // take `bytes` more for work already admitted (e.g. a merged pass that
   // needs more than its jobs' footprints) if they are free now; give them
   // back with release()
   bool take(uint64_t bytes) {
-    if (used_ > budget_ || bytes > budget_ - used_) return false;
+    if (used_ + external_ > budget_ || bytes > budget_ - used_ - external_) return false;
     used_ += bytes;
     return true;
   }
   // admit jobs in FIFO order while the head fits; returns admitted tickets
   std::vector<uint64_t> admit(size_t max_jobs = SIZE_MAX) {
     std::vector<uint64_t> out;
-    while (!q_.empty() && out.size() < max_jobs && q_.front().bytes <= budget_ - used_) {
+    while (!q_.empty() && out.size() < max_jobs && used_ + external_ <= budget_ &&
+           q_.front().bytes <= budget_ - used_ - external_) {
       used_ += q_.front().bytes;
       out.push_back(q_.front().ticket);
       q_.pop_front();
@@ -64,6 +69,7 @@ class AdmissionQueue {
   uint64_t budget_;
   uint64_t used_ = 0;
   uint64_t reserved_ = 0;
+  uint64_t external_ = 0;
   std::deque<Item> q_;
 };
 

@@ -23,9 +23,9 @@ int msm_host(int device, const uint64_t* scalars, const uint64_t* bases_xy, uint
   // (host::fq::msm_combine_windows) and the normalisation
   fe *ds = nullptr, *db = nullptr, *dwin = nullptr;
   uint64_t win[zk::MSM_MAX_WINDOWS * 16];
-  cudaError_t e = cudaMallocAsync((void**)&ds, n * 32, s);
-  if (e == cudaSuccess) e = cudaMallocAsync((void**)&db, n * 64, s);
-  if (e == cudaSuccess) e = cudaMallocAsync((void**)&dwin, zk::MSM_MAX_WINDOWS * 128, s);
+  cudaError_t e = zk::dmalloc((void**)&ds, n * 32, s);
+  if (e == cudaSuccess) e = zk::dmalloc((void**)&db, n * 64, s);
+  if (e == cudaSuccess) e = zk::dmalloc((void**)&dwin, zk::MSM_MAX_WINDOWS * 128, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(ds, scalars, n * 32, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(db, bases_xy, n * 64, cudaMemcpyHostToDevice, s);
   uint64_t nl = 0;

@@ -30,11 +30,11 @@ int ntt_device(int device, fe* d_a, uint32_t log_n, const hf::Fr& w, const hf::F
                cudaStream_t s) {
   (void)device;
   cudaError_t e;
-  const zk::NttTables* t = zk::ntt_tables_get(device, w, (int)log_n, s, &e);
+  const zk::NttTablesRef t = zk::ntt_tables_get(device, w, (int)log_n, s, &e);
   if (!t) return zk::status_of("ntt_tables_get", e);
   const size_t n = (size_t)1 << log_n;
   fe* tmp = nullptr;
-  if (t->plan.npass > 1) ZK_TRY("cudaMallocAsync(ntt scratch)", cudaMallocAsync((void**)&tmp, n * sizeof(fe), s));
+  if (t->plan.npass > 1) ZK_TRY("zk::dmalloc(ntt scratch)", zk::dmalloc((void**)&tmp, n * sizeof(fe), s));
   zk::PowTables pre;
   if (coset) {
     e = zk::pow_tables_make(&pre, *coset, (int)log_n, s);
@@ -60,7 +60,7 @@ int ntt_host(int device, uint64_t* a, uint32_t log_n, const uint64_t* omega, con
   if (st) return st;
   const size_t bytes = ((size_t)1 << log_n) * sizeof(fe);
   fe* d = nullptr;
-  ZK_TRY("cudaMallocAsync(ntt data)", cudaMallocAsync((void**)&d, bytes, s));
+  ZK_TRY("zk::dmalloc(ntt data)", zk::dmalloc((void**)&d, bytes, s));
   cudaError_t e = cudaMemcpyAsync(d, a, bytes, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) {
     st = ntt_device(device, d, log_n, load_fr(omega), coset, post, s);
@@ -90,20 +90,20 @@ int lde_device(int device, const fe* d_values, uint32_t log_n, fe* d_ext, uint32
   // 2) NTT of d_ext on the extended domain; its first pass treats the zero
   //    padding [n, N) as known zeros, so the tail is never written or read
   cudaError_t e;
-  const zk::NttTables* ti = zk::ntt_tables_get(device, w_inv, (int)log_n, s, &e);
+  const zk::NttTablesRef ti = zk::ntt_tables_get(device, w_inv, (int)log_n, s, &e);
   if (!ti) return zk::status_of("ntt_tables_get", e);
-  const zk::NttTables* te = zk::ntt_tables_get(device, w_ext, (int)log_ext, s, &e);
+  const zk::NttTablesRef te = zk::ntt_tables_get(device, w_ext, (int)log_ext, s, &e);
   if (!te) return zk::status_of("ntt_tables_get", e);
-  const zk::PowTables* gd = zk::pow_tables_get(device, g, (int)log_n, s, &e, &divisor);
+  const zk::PowTablesRef gd = zk::pow_tables_get(device, g, (int)log_n, s, &e, &divisor);
   if (!gd) return zk::status_of("pow_tables_get", e);
   fe* tmp = nullptr;
-  ZK_TRY("cudaMallocAsync(lde scratch)", cudaMallocAsync((void**)&tmp, N * sizeof(fe), s));
+  ZK_TRY("zk::dmalloc(lde scratch)", zk::dmalloc((void**)&tmp, N * sizeof(fe), s));
   // the skip works on whole rows of the first pass; otherwise zero the tail
   if (te->plan.npass > 1 && N > n && n % (1ull << (log_ext - te->plan.bits[0])) != 0)
     ZK_TRY("lde zero", cudaMemsetAsync(d_ext + n, 0, (N - n) * sizeof(fe), s));
   zk::NttFuse f1;
   f1.src = d_values;
-  f1.post_tab = gd;
+  f1.post_tab = gd.get();
   e = zk::ntt_run(*ti, d_ext, tmp, f1, s);
   zk::count_launches(ti->plan.npass);
   if (e == cudaSuccess) {
@@ -123,29 +123,29 @@ int ext_to_coeff_device(int device, const fe* d_ext, uint32_t log_ext, const hf:
                         const hf::Fr& g_inv, fe* d_out, uint64_t m, cudaStream_t s) {
   const size_t N = (size_t)1 << log_ext;
   cudaError_t e;
-  const zk::NttTables* t = zk::ntt_tables_get(device, w_inv, (int)log_ext, s, &e);
+  const zk::NttTablesRef t = zk::ntt_tables_get(device, w_inv, (int)log_ext, s, &e);
   if (!t) return zk::status_of("ntt_tables_get", e);
   const bool tiny = t->plan.npass == 0;  // direct kernel: constant scale only
-  const zk::PowTables* gd = zk::pow_tables_get(device, g_inv, (int)log_ext, s, &e, tiny ? nullptr : &divisor);
+  const zk::PowTablesRef gd = zk::pow_tables_get(device, g_inv, (int)log_ext, s, &e, tiny ? nullptr : &divisor);
   if (!gd) return zk::status_of("pow_tables_get", e);
   fe *work = nullptr, *tmp = nullptr;
-  ZK_TRY("cudaMallocAsync(ext_to_coeff work)", cudaMallocAsync((void**)&work, N * sizeof(fe), s));
+  ZK_TRY("zk::dmalloc(ext_to_coeff work)", zk::dmalloc((void**)&work, N * sizeof(fe), s));
   if (t->plan.npass > 1) {
-    e = cudaMallocAsync((void**)&tmp, N * sizeof(fe), s);
+    e = zk::dmalloc((void**)&tmp, N * sizeof(fe), s);
     if (e != cudaSuccess) {
       cudaFreeAsync(work, s);
-      return zk::status_of("cudaMallocAsync(ext_to_coeff scratch)", e);
+      return zk::status_of("zk::dmalloc(ext_to_coeff scratch)", e);
     }
   }
   if (tiny) {
     e = cudaMemcpyAsync(work, d_ext, N * sizeof(fe), cudaMemcpyDeviceToDevice, s);
     if (e == cudaSuccess) e = zk::ntt_run(*t, work, tmp, nullptr, &divisor, s);
-    if (e == cudaSuccess) e = zk::fr_scale_copy(d_out, work, m, 1, gd, s);
+    if (e == cudaSuccess) e = zk::fr_scale_copy(d_out, work, m, 1, gd.get(), s);
     zk::count_launches(2);
   } else {
     zk::NttFuse f;
     f.src = d_ext;
-    f.post_tab = gd;
+    f.post_tab = gd.get();
     e = zk::ntt_run(*t, work, tmp, f, s);
     zk::count_launches(t->plan.npass);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_out, work, m * sizeof(fe), cudaMemcpyDeviceToDevice, s);
@@ -243,11 +243,11 @@ extern "C" int zkgpu_lagrange_to_extended(int device, const uint64_t* values, ui
   if (st) return st;
   const size_t n = (size_t)1 << log_n, N = (size_t)1 << log_ext;
   fe *d_in = nullptr, *d_ext = nullptr;
-  ZK_TRY("cudaMallocAsync(lde in)", cudaMallocAsync((void**)&d_in, n * sizeof(fe), s));
-  cudaError_t e = cudaMallocAsync((void**)&d_ext, N * sizeof(fe), s);
+  ZK_TRY("zk::dmalloc(lde in)", zk::dmalloc((void**)&d_in, n * sizeof(fe), s));
+  cudaError_t e = zk::dmalloc((void**)&d_ext, N * sizeof(fe), s);
   if (e != cudaSuccess) {
     cudaFreeAsync(d_in, s);
-    return zk::status_of("cudaMallocAsync(lde ext)", e);
+    return zk::status_of("zk::dmalloc(lde ext)", e);
   }
   e = cudaMemcpyAsync(d_in, values, n * sizeof(fe), cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) {
@@ -312,11 +312,11 @@ extern "C" int zkgpu_extended_to_coeff(int device, const uint64_t* ext, uint32_t
   if (st) return st;
   const size_t N = (size_t)1 << log_ext;
   fe *d_ext = nullptr, *d_out = nullptr;
-  ZK_TRY("cudaMallocAsync(ext_to_coeff in)", cudaMallocAsync((void**)&d_ext, N * sizeof(fe), s));
-  cudaError_t e = cudaMallocAsync((void**)&d_out, m * sizeof(fe), s);
+  ZK_TRY("zk::dmalloc(ext_to_coeff in)", zk::dmalloc((void**)&d_ext, N * sizeof(fe), s));
+  cudaError_t e = zk::dmalloc((void**)&d_out, m * sizeof(fe), s);
   if (e != cudaSuccess) {
     cudaFreeAsync(d_ext, s);
-    return zk::status_of("cudaMallocAsync(ext_to_coeff out)", e);
+    return zk::status_of("zk::dmalloc(ext_to_coeff out)", e);
   }
   e = cudaMemcpyAsync(d_ext, ext, N * sizeof(fe), cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) {
@@ -377,9 +377,9 @@ extern "C" int zkgpu_field_op(int device, int op, int fid, const uint64_t* a, co
   if (st) return st;
   const size_t bytes = n * sizeof(fe);
   fe *da = nullptr, *db = nullptr, *dout = nullptr;
-  ZK_TRY("cudaMallocAsync", cudaMallocAsync((void**)&da, bytes, s));
-  ZK_TRY("cudaMallocAsync", cudaMallocAsync((void**)&db, bytes, s));
-  ZK_TRY("cudaMallocAsync", cudaMallocAsync((void**)&dout, bytes, s));
+  ZK_TRY("cudaMallocAsync", zk::dmalloc((void**)&da, bytes, s));
+  ZK_TRY("cudaMallocAsync", zk::dmalloc((void**)&db, bytes, s));
+  ZK_TRY("cudaMallocAsync", zk::dmalloc((void**)&dout, bytes, s));
   cudaMemcpyAsync(da, a, bytes, cudaMemcpyHostToDevice, s);
   cudaMemcpyAsync(db, b, bytes, cudaMemcpyHostToDevice, s);
   const unsigned grid = (unsigned)((n + 255) / 256);

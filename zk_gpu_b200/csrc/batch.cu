@@ -21,40 +21,6 @@
 
 namespace zk {
 
-namespace {
-struct PowKey {
-  int dev, log_n;
-  uint64_t c[4], s[4];
-  bool operator<(const PowKey& o) const {
-    return std::tie(dev, log_n, c[0], c[1], c[2], c[3], s[0], s[1], s[2], s[3]) <
-           std::tie(o.dev, o.log_n, o.c[0], o.c[1], o.c[2], o.c[3], o.s[0], o.s[1], o.s[2], o.s[3]);
-  }
-};
-std::mutex g_pow_mu;
-std::map<PowKey, PowTables> g_pow_cache;
-}  // namespace
-
-// Coset power tables cached per (device, c, log_n): batches and the serving
-// loop reuse the same few cosets (the field generator and its shifts).
-const PowTables* pow_tables_get(int device, const host::Fr& c, int log_n, cudaStream_t s, cudaError_t* err,
-                                const host::Fr* scale) {
-  const host::Fr one = host::one();
-  const host::Fr& sc = scale ? *scale : one;
-  PowKey k{device, log_n, {c.v[0], c.v[1], c.v[2], c.v[3]}, {sc.v[0], sc.v[1], sc.v[2], sc.v[3]}};
-  std::lock_guard<std::mutex> lk(g_pow_mu);
-  auto it = g_pow_cache.find(k);
-  if (it != g_pow_cache.end()) {
-    *err = cudaSuccess;
-    return &it->second;
-  }
-  PowTables t;
-  cudaError_t e = pow_tables_make(&t, c, log_n, s, scale);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  *err = e;
-  if (e != cudaSuccess) return nullptr;
-  return &g_pow_cache.emplace(k, t).first->second;
-}
-
 struct NttBatch {
   int device = 0;
   BatchPass* d_passes = nullptr;
@@ -65,6 +31,9 @@ struct NttBatch {
   cudaGraphExec_t exec = nullptr;
   int grid = 0;
   uint64_t launches_per_run = 2;
+  // tables the graph's passes read, held for the batch's lifetime
+  std::vector<NttTablesRef> tables;
+  std::vector<PowTablesRef> pows;
   ~NttBatch() {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
@@ -95,8 +64,8 @@ extern "C" int zkgpu_ntt_batch_create(int device, const zkgpu_ntt_job* jobs, uin
   b->device = device;
   // validate and collect per-job tables
   struct JobInfo {
-    const zk::NttTables* t;
-    const zk::PowTables* pre;
+    zk::NttTablesRef t;
+    zk::PowTablesRef pre;
     hf::Fr post;
     bool has_post;
     size_t tmp_off;
@@ -127,6 +96,8 @@ extern "C" int zkgpu_ntt_batch_create(int device, const zkgpu_ntt_job* jobs, uin
     info[j].tmp_off = tmp_elems;
     if (info[j].t->plan.npass > 1) tmp_elems += (size_t)1 << jb.log_n;
     if (info[j].t->plan.npass > max_pass) max_pass = info[j].t->plan.npass;
+    b->tables.push_back(info[j].t);
+    if (info[j].pre) b->pows.push_back(info[j].pre);
   }
   if (tmp_elems) ZK_TRY("cudaMalloc(batch scratch)", cudaMalloc((void**)&b->d_tmp, tmp_elems * sizeof(fe)));
   // level-ordered pass list
@@ -139,7 +110,7 @@ extern "C" int zkgpu_ntt_batch_create(int device, const zkgpu_ntt_job* jobs, uin
       if (lvl >= t.plan.npass) continue;
       zk::BatchPass bp{};
       const uint64_t ncta = zk::ntt_pass_params(t, lvl, reinterpret_cast<fe*>(jobs[j].data), b->d_tmp + info[j].tmp_off,
-                                                info[j].pre, info[j].has_post ? &info[j].post : nullptr, &bp.p);
+                                                info[j].pre.get(), info[j].has_post ? &info[j].post : nullptr, &bp.p);
       bp.B = (uint32_t)t.plan.bits[lvl];
       bp.ntiles = (uint32_t)ncta;
       bp.tile_base = (uint32_t)tiles;
@@ -218,7 +189,7 @@ extern "C" int zkgpu_selftest_wait_timeout(int device, const uint64_t omega12[4]
   hf::Fr w = fr_of(omega12);
   if (!hf::is_canonical(w) || !hf::is_primitive_root(w, L)) return ZKGPU_EINVAL;
   cudaError_t e;
-  const zk::NttTables* t = zk::ntt_tables_get(device, w, L, s, &e);
+  const zk::NttTablesRef t = zk::ntt_tables_get(device, w, L, s, &e);
   if (!t) return zk::status_of("ntt_tables_get", e);
   if (t->plan.npass != 2) return ZKGPU_EINVAL;
   fe *d = nullptr, *tmp = nullptr;

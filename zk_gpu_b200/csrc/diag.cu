@@ -118,7 +118,7 @@ extern "C" int zkgpu_int_peak(int device, uint32_t iters, double* imad_per_s, do
   int sms = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   uint32_t* sink = nullptr;
-  ZK_TRY("cudaMalloc", cudaMallocAsync((void**)&sink, 4096 * 4, s));
+  ZK_TRY("cudaMalloc", zk::dmalloc((void**)&sink, 4096 * 4, s));
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);

@@ -122,8 +122,8 @@ extern "C" int zkgpu_g1_mul_fixed_dev(int device, const uint64_t base_xy[8], con
   if (st) return st;
   cudaStream_t s = (cudaStream_t)stream;
   fe *d_base = nullptr, *d_table = nullptr;
-  cudaError_t e = cudaMallocAsync((void**)&d_base, 64, s);
-  if (e == cudaSuccess) e = cudaMallocAsync((void**)&d_table, 64 * 16 * 64, s);
+  cudaError_t e = zk::dmalloc((void**)&d_base, 64, s);
+  if (e == cudaSuccess) e = zk::dmalloc((void**)&d_table, 64 * 16 * 64, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(d_base, base_xy, 64, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) {
     zk::g1_fixed_table_kernel<<<1, 64, 0, s>>>(d_base, d_table);

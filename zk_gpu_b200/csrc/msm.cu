@@ -4,6 +4,7 @@
 #include "curve.cuh"
 #include "msm.cuh"
 #include "prof.cuh"
+#include "runtime.cuh"
 
 namespace zk {
 
@@ -698,7 +699,7 @@ cudaError_t msm_run_impl(const fe* d_scalars, const fe* d_bases, uint64_t n, fe*
   uint32_t *nch = nullptr, *heavy = nullptr, *heavy_count = nullptr;
   cudaError_t e = cudaSuccess;
   auto alloc = [&](void** ptr, size_t bytes) {
-    if (e == cudaSuccess) e = cudaMallocAsync(ptr, bytes ? bytes : 4, s);
+    if (e == cudaSuccess) e = zk::dmalloc(ptr, bytes ? bytes : 4, s);
   };
   alloc((void**)&counts, T * 4ull);
   alloc((void**)&offsets, (T + 1ull) * 4);

@@ -23,6 +23,7 @@
 #include "ntt.cuh"
 #include "ntt_tile.cuh"
 #include "prof.cuh"
+#include "runtime.cuh"
 
 namespace zk {
 
@@ -215,10 +216,11 @@ static cudaError_t pow_two_level(fe** lo, fe** hi, uint32_t* shift, const host::
   const uint32_t sh = (uint32_t)((log_count + 1) / 2);
   const uint64_t nlo = 1ull << sh, nhi = 1ull << (log_count > (int)sh ? log_count - sh : 0);
   cudaError_t e;
+  *lo = *hi = nullptr;
   if (pooled) {
-    e = cudaMallocAsync((void**)lo, nlo * sizeof(fe), s);
+    e = zk::dmalloc((void**)lo, nlo * sizeof(fe), s);
     if (e != cudaSuccess) return e;
-    e = cudaMallocAsync((void**)hi, nhi * sizeof(fe), s);
+    e = zk::dmalloc((void**)hi, nhi * sizeof(fe), s);
     if (e != cudaSuccess) return e;
   } else {
     e = cudaMalloc((void**)lo, nlo * sizeof(fe));
@@ -244,8 +246,9 @@ __global__ void scale_table_kernel(fe* t, fe scale, uint64_t count) {
   st_fe(t + i, v);
 }
 
-cudaError_t pow_tables_make(PowTables* t, const host::Fr& c, int log_n, cudaStream_t s, const host::Fr* scale) {
-  cudaError_t e = pow_two_level(&t->lo, &t->hi, &t->shift, c, log_n, s, true);
+cudaError_t pow_tables_make(PowTables* t, const host::Fr& c, int log_n, cudaStream_t s, const host::Fr* scale,
+                            bool pooled) {
+  cudaError_t e = pow_two_level(&t->lo, &t->hi, &t->shift, c, log_n, s, pooled);
   if (e == cudaSuccess && scale) {
     const uint64_t nlo = 1ull << t->shift;
     scale_table_kernel<<<(unsigned)((nlo + 255) / 256), 256, 0, s>>>(t->lo, to_fe_rp(*scale), nlo);
@@ -258,26 +261,6 @@ void pow_tables_free(PowTables* t, cudaStream_t s) {
   if (t->hi) cudaFreeAsync(t->hi, s);
   t->lo = t->hi = nullptr;
 }
-
-namespace {
-struct Key {
-  int dev;
-  int log_n;
-  uint64_t w[4];
-  uint32_t plan;  // pass widths, 6 bits each
-  bool operator<(const Key& o) const {
-    return std::tie(dev, log_n, w[0], w[1], w[2], w[3], plan) <
-           std::tie(o.dev, o.log_n, o.w[0], o.w[1], o.w[2], o.w[3], o.plan);
-  }
-};
-uint32_t plan_code(const NttPlan& p) {
-  uint32_t c = (uint32_t)p.npass;
-  for (int k = 0; k < NTT_MAX_PASS; k++) c = (c << 6) | (uint32_t)p.bits[k];
-  return c;
-}
-std::mutex g_mu;
-std::map<Key, std::unique_ptr<NttTables>> g_cache;
-}  // namespace
 
 static cudaError_t build_tables(NttTables* t, cudaStream_t s) {
   const NttPlan& p = t->plan;
@@ -401,29 +384,6 @@ void ntt_tables_release(NttTables* t) {
     t->inner[k] = t->twist[k] = nullptr;
   }
   t->bytes = 0;
-}
-
-const NttTables* ntt_tables_get(int device, const host::Fr& omega, int log_n, cudaStream_t s, cudaError_t* err) {
-  // the plan is the autotuner's choice for this device and size, if any;
-  // tables of a plan stay cached after the choice changes (work may still use them)
-  const NttPlan plan = tuned_ntt_plan(device, log_n);
-  Key key{device, log_n, {omega.v[0], omega.v[1], omega.v[2], omega.v[3]}, plan_code(plan)};
-  std::lock_guard<std::mutex> lk(g_mu);
-  auto it = g_cache.find(key);
-  if (it != g_cache.end()) {
-    *err = cudaSuccess;
-    return it->second.get();
-  }
-  auto t = std::make_unique<NttTables>();
-  cudaError_t e = ntt_tables_build(t.get(), plan, omega, s);
-  if (e != cudaSuccess) {
-    *err = e;
-    return nullptr;
-  }
-  *err = cudaSuccess;
-  const NttTables* res = t.get();
-  g_cache.emplace(key, std::move(t));
-  return res;
 }
 
 static cudaError_t dispatch_pass(int B, const PassParams& pp, uint64_t ncta, cudaStream_t s) {

@@ -18,6 +18,7 @@
 
 #include <cstdint>
 #include <cstddef>
+#include <memory>
 
 #include "field.cuh"
 #include "host_field.hpp"
@@ -57,9 +58,15 @@ struct PowTables {
   uint32_t shift = 0;
 };
 
-// Cached tables for (device, omega, log_n); thread-safe.  Returns nullptr and
-// sets *err on failure.  The cache owns the memory.
-const NttTables* ntt_tables_get(int device, const host::Fr& omega, int log_n, cudaStream_t s, cudaError_t* err);
+// Cached tables for (device, omega, log_n) under the device's current plan;
+// thread-safe.  Returns null and sets *err on failure.  The reference keeps
+// the tables alive: work that reads them (an enqueued transform, a batch
+// graph, a serving wave) holds it until the work is done or destroyed.  The
+// cache is capped per device (ZKGPU_TABLE_CACHE_MB, default 8192) and evicts
+// its least recently used entries; an evicted table is freed when its last
+// holder lets go (cudaFree, which waits for the device).
+using NttTablesRef = std::shared_ptr<const NttTables>;
+NttTablesRef ntt_tables_get(int device, const host::Fr& omega, int log_n, cudaStream_t s, cudaError_t* err);
 // Uncached tables for an explicit plan (the autotuner's trials); free with
 // ntt_tables_release after the work using them has finished.
 cudaError_t ntt_tables_build(NttTables* t, const NttPlan& plan, const host::Fr& omega, cudaStream_t s);
@@ -69,14 +76,20 @@ void ntt_tables_release(NttTables* t);
 size_t ntt_tables_elems(int log_n);
 cudaError_t ntt_tables_fill(NttTables* t, const host::Fr& omega, int log_n, fe* mem, size_t cap, cudaStream_t s);
 // Two-level power tables for scale * c^x, x < 2^log_n (scale folded into the
-// low table; null = 1), allocated from the stream pool (caller frees with
-// pow_tables_free on the same stream).
+// low table; null = 1), allocated from the library pool on `s` (caller frees
+// with pow_tables_free on the same stream), or with cudaMalloc when !pooled.
 cudaError_t pow_tables_make(PowTables* t, const host::Fr& c, int log_n, cudaStream_t s,
-                            const host::Fr* scale = nullptr);
+                            const host::Fr* scale = nullptr, bool pooled = true);
 void pow_tables_free(PowTables* t, cudaStream_t s);
-// Cached (device, c, log_n, scale) power tables, owned by the cache.
-const PowTables* pow_tables_get(int device, const host::Fr& c, int log_n, cudaStream_t s, cudaError_t* err,
-                                const host::Fr* scale = nullptr);
+// Cached (device, c, log_n, scale) power tables, under the same cap and
+// lifetime rules as ntt_tables_get.
+using PowTablesRef = std::shared_ptr<const PowTables>;
+PowTablesRef pow_tables_get(int device, const host::Fr& c, int log_n, cudaStream_t s, cudaError_t* err,
+                            const host::Fr* scale = nullptr);
+// Bytes the device's table caches hold, and dropping every cached entry
+// (entries still held by work stay alive until it lets go).
+uint64_t table_cache_bytes(int device);
+void table_cache_clear(int device);
 
 // Parameters of one pass launch (kernel argument / batch descriptor).
 struct PassParams {

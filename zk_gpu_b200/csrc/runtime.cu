@@ -20,8 +20,47 @@ struct ThreadStreams {
 };
 thread_local ThreadStreams t_streams;
 std::mutex g_pool_mu;
-std::vector<bool> g_pool_done;
+std::vector<cudaMemPool_t> g_pools;  // the library's pool per device, created on first use
 }  // namespace
+
+static cudaError_t library_pool(int device, cudaMemPool_t* out) {
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if ((int)g_pools.size() <= device) g_pools.resize(device + 1, nullptr);
+  if (!g_pools[device]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t pool;
+    cudaError_t e = cudaMemPoolCreate(&pool, &props);
+    if (e != cudaSuccess) return e;
+    uint64_t thr = UINT64_MAX;  // keep freed blocks for the next call instead of returning them
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    g_pools[device] = pool;
+  }
+  *out = g_pools[device];
+  return cudaSuccess;
+}
+
+cudaError_t dmalloc(void** ptr, size_t bytes, cudaStream_t s) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  cudaMemPool_t pool;
+  e = library_pool(dev, &pool);
+  if (e != cudaSuccess) return e;
+  return cudaMallocFromPoolAsync(ptr, bytes, pool, s);
+}
+
+cudaError_t trim_pool(int device) {
+  cudaMemPool_t pool = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (device < (int)g_pools.size()) pool = g_pools[device];
+  }
+  return pool ? cudaMemPoolTrimTo(pool, 0) : cudaSuccess;
+}
 
 void set_last_error(const char* where, cudaError_t e) {
   std::snprintf(t_err, sizeof(t_err), "%s: %s (%d)", where, cudaGetErrorString(e), (int)e);
@@ -49,18 +88,6 @@ int bind_device(int device, cudaStream_t* stream) {
     return ZKGPU_ENODEV;
   }
   ZK_TRY("cudaSetDevice", cudaSetDevice(device));
-  {
-    std::lock_guard<std::mutex> lk(g_pool_mu);
-    if ((int)g_pool_done.size() < count) g_pool_done.resize(count, false);
-    if (!g_pool_done[device]) {
-      cudaMemPool_t pool;
-      if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
-        uint64_t thr = UINT64_MAX;
-        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
-      }
-      g_pool_done[device] = true;
-    }
-  }
   if ((int)t_streams.by_dev.size() < count) t_streams.by_dev.resize(count, nullptr);
   if (!t_streams.by_dev[device]) {
     cudaStream_t s;

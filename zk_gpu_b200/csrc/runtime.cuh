@@ -21,9 +21,21 @@ void count_launches(uint64_t k);
 int status_of(const char* where, cudaError_t e);
 
 // Make `device` current on this thread and return this thread's work stream
-// for it (created once, non-blocking).  The device's default memory pool is
-// configured to keep freed memory cached.
+// for it (created once, non-blocking).
 int bind_device(int device, cudaStream_t* stream);
+
+// Stream-ordered device allocation from the library's own memory pool on the
+// current device (created on first use).  The pool keeps freed memory cached
+// for reuse by later calls; the process's default pool, which the caller's
+// own allocations may use, is left as the caller configured it.  Free with
+// cudaFreeAsync.  zkgpu_release_cached returns the cached memory.
+cudaError_t dmalloc(void** ptr, size_t bytes, cudaStream_t s);
+// Return the library pool's cached, unused memory on `device` to the system.
+cudaError_t trim_pool(int device);
+template <class T>
+inline cudaError_t dmalloc(T** ptr, size_t bytes, cudaStream_t s) {
+  return dmalloc(reinterpret_cast<void**>(ptr), bytes, s);
+}
 
 }  // namespace zk
 

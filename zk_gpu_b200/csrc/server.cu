@@ -60,6 +60,7 @@ struct Wave {
   cudaStream_t s_ntt = nullptr, s_msm = nullptr;
   cudaEvent_t ev_ntt = nullptr, ev_msm = nullptr;
   std::vector<BatchPass> passes;  // host copy kept alive for the async upload
+  std::vector<std::shared_ptr<const void>> tables;  // tables the wave's passes read, held until it retires
   uint64_t* mailbox = nullptr;    // pinned: [0] batch error flag, then kMsmSlotWords per MSM job
   uint64_t extra_bytes = 0;       // budget taken beyond the jobs' footprints (merged MSM passes)
   int status = ZKGPU_OK;
@@ -182,7 +183,7 @@ class Server {
     o->waves = waves_;
     o->batch_launches = batch_launches_;
     o->hbm_budget = adm_.budget() + adm_.reserved();
-    o->hbm_used = adm_.used() + adm_.reserved();
+    o->hbm_used = adm_.used() + adm_.reserved() + adm_.external();
     o->hbm_peak = peak_;
     o->pending = adm_.pending();
     o->inflight = inflight_jobs_;
@@ -214,9 +215,18 @@ class Server {
         });
         if (stop_) return;
         const uint64_t gen = retired_gen_;
+        // the device's table caches count against the budget too
+        adm_.set_external(table_cache_bytes(device_));
         for (uint64_t t : adm_.admit(max_wave_)) batch.push_back(jobs_.at(t).get());
-        peak_ = std::max(peak_, adm_.used() + adm_.reserved());
+        peak_ = std::max(peak_, adm_.used() + adm_.reserved() + adm_.external());
         if (batch.empty()) {
+          if (waves_inflight_ == 0 && adm_.external() > 0) {
+            // nothing will retire to make room: drop the cached tables (work
+            // still holding some keeps them alive) and try again
+            lk.unlock();
+            table_cache_clear(device_);
+            continue;
+          }
           // the head does not fit yet: wait until a wave retires and frees memory
           cv_sched_.wait(lk, [&] { return stop_ || retired_gen_ != gen; });
           continue;
@@ -252,13 +262,13 @@ class Server {
     w.mailbox[0] = 0;
     uint64_t* next_msm_slot = w.mailbox + 2;
     struct NttItem {
-      const NttTables* t;
+      NttTablesRef t;
       fe* data;
       fe* tmp;
-      const PowTables* pre;
+      PowTablesRef pre;
       host::Fr post;
       bool has_post;
-      const PowTables* post_tab;  // final pass: output i times table power i
+      PowTablesRef post_tab;  // final pass: output i times table power i
       uint64_t nonzero;           // first pass: inputs past this are zero padding
       int level0;
       int dep_job;  // index in items of the transform this one follows, or -1
@@ -295,7 +305,7 @@ class Server {
           ok_merge = adm_.take(need - admitted);
           if (ok_merge) {
             w.extra_bytes += need - admitted;
-            peak_ = std::max(peak_, adm_.used() + adm_.reserved());
+            peak_ = std::max(peak_, adm_.used() + adm_.reserved() + adm_.external());
           }
         }
       }
@@ -315,9 +325,9 @@ class Server {
       const uint64_t n_total = off.back();
       fe *ds = nullptr, *dwin = nullptr;
       uint32_t* doff = nullptr;
-      if (ok(cudaMallocAsync((void**)&ds, std::max<uint64_t>(n_total, 1) * 32, w.s_msm)) &&
-          ok(cudaMallocAsync((void**)&dwin, grp.size() * MSM_MAX_WINDOWS * 128, w.s_msm)) &&
-          ok(cudaMallocAsync((void**)&doff, off.size() * 4, w.s_msm))) {
+      if (ok(zk::dmalloc((void**)&ds, std::max<uint64_t>(n_total, 1) * 32, w.s_msm)) &&
+          ok(zk::dmalloc((void**)&dwin, grp.size() * MSM_MAX_WINDOWS * 128, w.s_msm)) &&
+          ok(zk::dmalloc((void**)&doff, off.size() * 4, w.s_msm))) {
         // offsets travel through the wave's pinned mailbox tail so the copy
         // stays asynchronous
         uint32_t* h_off = reinterpret_cast<uint32_t*>(next_msm_slot);
@@ -356,8 +366,8 @@ class Server {
         // does the Horner step on the host (host::fq::msm_combine_windows)
         fe *ds = nullptr, *dwin = nullptr;
         const BaseSet& bs = bases_[j.bases_id];
-        if (ok(cudaMallocAsync((void**)&ds, std::max<uint64_t>(j.n, 1) * 32, w.s_msm)) &&
-            ok(cudaMallocAsync((void**)&dwin, MSM_MAX_WINDOWS * 128, w.s_msm)) &&
+        if (ok(zk::dmalloc((void**)&ds, std::max<uint64_t>(j.n, 1) * 32, w.s_msm)) &&
+            ok(zk::dmalloc((void**)&dwin, MSM_MAX_WINDOWS * 128, w.s_msm)) &&
             ok(cudaMemcpyAsync(ds, j.input, j.n * 32, cudaMemcpyHostToDevice, w.s_msm))) {
           uint64_t nl = 0;
           MsmWindowsOut wo;
@@ -378,7 +388,7 @@ class Server {
       const uint32_t L = lde ? j.log_ext : j.log_n;
       const size_t N = (size_t)1 << L, n = (size_t)1 << j.log_n;
       fe *d = nullptr, *tmp = nullptr;
-      if (!ok(cudaMallocAsync((void**)&d, N * 32, w.s_ntt)) || !ok(cudaMallocAsync((void**)&tmp, N * 32, w.s_ntt)))
+      if (!ok(zk::dmalloc((void**)&d, N * 32, w.s_ntt)) || !ok(zk::dmalloc((void**)&tmp, N * 32, w.s_ntt)))
         break;
       frees_ntt.push_back(d);
       frees_ntt.push_back(tmp);
@@ -446,9 +456,9 @@ class Server {
           if (k < 0 || k >= it.t->plan.npass) continue;
           BatchPass bp{};
           NttFuse fu;
-          fu.pre = it.pre;
+          fu.pre = it.pre.get();
           fu.post = it.has_post ? &it.post : nullptr;
-          fu.post_tab = it.post_tab;
+          fu.post_tab = it.post_tab.get();
           fu.nonzero = it.nonzero;
           const uint64_t ncta = ntt_pass_params(*it.t, k, it.data, it.tmp, fu, &bp.p);
           bp.B = (uint32_t)it.t->plan.bits[k];
@@ -465,8 +475,8 @@ class Server {
       BatchPass* dp = nullptr;
       uint32_t* dc = nullptr;
       const size_t np = w.passes.size();
-      if (ok(cudaMallocAsync((void**)&dp, np * sizeof(BatchPass), w.s_ntt)) &&
-          ok(cudaMallocAsync((void**)&dc, (2 + np) * 4, w.s_ntt)) &&
+      if (ok(zk::dmalloc((void**)&dp, np * sizeof(BatchPass), w.s_ntt)) &&
+          ok(zk::dmalloc((void**)&dc, (2 + np) * 4, w.s_ntt)) &&
           ok(cudaMemcpyAsync(dp, w.passes.data(), np * sizeof(BatchPass), cudaMemcpyHostToDevice, w.s_ntt)) &&
           ok(cudaMemsetAsync(dc, 0, (2 + np) * 4, w.s_ntt))) {
         ok(ntt_batch_launch(dp, (uint32_t)np, (uint32_t)tiles, dc, dc + 2, dc + 1, grid_, w.s_ntt));
@@ -480,6 +490,11 @@ class Server {
         const uint32_t L = j.kind == ZKGPU_KIND_LDE ? j.log_ext : j.log_n;
         ok(cudaMemcpyAsync(j.output, o.second, ((size_t)1 << L) * 32, cudaMemcpyDeviceToHost, w.s_ntt));
       }
+    }
+    for (const NttItem& it : items) {
+      w.tables.push_back(it.t);
+      if (it.pre) w.tables.push_back(it.pre);
+      if (it.post_tab) w.tables.push_back(it.post_tab);
     }
     for (void* p : frees_ntt)
       if (p) cudaFreeAsync(p, w.s_ntt);
