@@ -732,25 +732,29 @@ def bench_serving(zk, torch, dev: int, njobs: int = 1000, rate: float = 2000.0, 
     lat_pc, span_pc = run_plain(None)
     st = srv.stats()
     one_cap = n / span_pc
-    # ---- equal p99: the one-call arm at 80% of its saturation rate sets the
-    # p99 budget; the serving loop's largest sustained rate within it ----
-    lam1 = 0.8 * one_cap
-    lat_p1, span_p1 = run_plain(lam1)
-    p99_budget = pct(lat_p1, 99)
-    # a rate is sustained at equal p99 when the serving loop's p99 stays within
-    # the one-call arm's (a backlog would grow the p99 without bound)
+    # ---- equal p99: each arm's p99 latency over a sweep of offered rates on
+    # the same Poisson trace; for every p99 the one-call arm reaches, the
+    # largest rate the serving loop sustains within that p99 ----
+    one_curve = []
+    for frac in (0.5, 0.7, 0.8, 0.9, 0.95):
+        lat_x, span_x = run_plain(frac * one_cap)
+        one_curve.append({"offered_jobs_s": round(frac * one_cap, 1), "achieved_jobs_s": round(n / span_x, 1),
+                          "p50_ms": round(pct(lat_x, 50) * 1e3, 2), "p99_ms": round(pct(lat_x, 99) * 1e3, 2)})
     sweep = []
-    best = None
-    for mult in (1.0, 2.0, 2.5, 3.0, 3.5, 4.0, 5.0, 6.0, 8.0):
-        lam = lam1 * mult
+    for mult in (0.5, 1.0, 1.5, 2.0, 2.5, 3.0, 3.5, 4.0):
+        lam = one_cap * mult
         lat_b, span_b = run_server(lam)
-        rec = {"offered_jobs_s": round(lam, 1), "achieved_jobs_s": round(n / span_b, 1),
-               "p50_ms": round(pct(lat_b, 50) * 1e3, 2), "p99_ms": round(pct(lat_b, 99) * 1e3, 2)}
-        sweep.append(rec)
-        if pct(lat_b, 99) <= p99_budget:
-            best = rec
-        else:
+        sweep.append({"offered_jobs_s": round(lam, 1), "achieved_jobs_s": round(n / span_b, 1),
+                      "p50_ms": round(pct(lat_b, 50) * 1e3, 2), "p99_ms": round(pct(lat_b, 99) * 1e3, 2)})
+        if pct(lat_b, 99) > 4 * max(r["p99_ms"] for r in one_curve) / 1e3:
             break
+    at_p99 = []
+    for r in one_curve:
+        ok = [b for b in sweep if b["p99_ms"] <= r["p99_ms"]]
+        best = max(ok, key=lambda b: b["offered_jobs_s"]) if ok else None
+        at_p99.append({"p99_ms": r["p99_ms"], "one_call_jobs_s": r["offered_jobs_s"],
+                       "batched_jobs_s": best["offered_jobs_s"] if best else None,
+                       "ratio": round(best["offered_jobs_s"] / r["offered_jobs_s"], 3) if best else None})
     # ---- verification: every job, batched (in waves, own buffers) vs alone ----
     verified, checked, chunk = 0, 0, []
     arena_bytes = 4 << 30
@@ -826,13 +830,10 @@ def bench_serving(zk, torch, dev: int, njobs: int = 1000, rate: float = 2000.0, 
                  "batched_closed_loop_d2h_gbs": round(d2h / span_sc / 1e9, 2),
                  "batched_closed_loop_h2d_gbs": round(h2d / span_sc / 1e9, 2),
                  "one_call_closed_loop_d2h_gbs": round(d2h / span_pc / 1e9, 2)})
-    eq = {"p99_budget_ms": round(p99_budget * 1e3, 2),
-          "one_call": {"offered_jobs_s": round(lam1, 1), "achieved_jobs_s": round(n / span_p1, 1),
-                       "p50_ms": round(pct(lat_p1, 50) * 1e3, 2), "p99_ms": round(p99_budget * 1e3, 2)},
-          "batched": best,
-          "jobs_s_ratio": round(best["offered_jobs_s"] / lam1, 3) if best else None,
-          "rule": "same Poisson trace; the serving loop's largest offered rate with p99 <= the one-call arm's "
-                  "p99 at 80% of its saturation throughput; ratio of offered rates"}
+    eq = {"rule": "same Poisson trace at each offered rate; for each p99 the one-call arm reaches (at 50-95% of "
+                  "its saturation throughput), the largest swept offered rate at which the serving loop's p99 is "
+                  "no higher; ratio of offered rates",
+          "at_p99": at_p99, "one_call_curve": one_curve}
     return {
         "jobs": n, "offered_rate_jobs_s": rate,
         "mix": "35% NTT 2^12-2^22, 35% coset LDE x4 2^12-2^22, 30% MSM 2^14-2^20 (resident 2^20 bases)",
@@ -847,7 +848,7 @@ def bench_serving(zk, torch, dev: int, njobs: int = 1000, rate: float = 2000.0, 
             "batched_jobs_s": round(n / span_sc, 1), "one_call_per_job_jobs_s": round(one_cap, 1),
             "speedup": round(span_pc / span_sc, 3),
             "batched_p99_ms": round(pct(lat_sc, 99) * 1e3, 3), "one_call_p99_ms": round(pct(lat_pc, 99) * 1e3, 3)},
-        "equal_p99": eq, "batched_rate_sweep": sweep,
+        "equal_p99": eq, "batched_rate_sweep": sweep, "eager_waves": os.environ.get("ZKGPU_SERVER_EAGER_WAVES", "2"),
         "server": {"waves": st["waves"], "batch_launches": st["batch_launches"], "hbm_peak_gb":
                    round(st["hbm_peak"] / 1e9, 2), "rejected": st["rejected"], "failed": st_after["failed"],
                    "msm_merged_passes": st_after["msm_merged_passes"],

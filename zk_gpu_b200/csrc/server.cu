@@ -13,6 +13,7 @@
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <memory>
@@ -75,7 +76,11 @@ struct BaseSet {
 
 class Server {
  public:
-  Server(int dev, uint64_t budget, uint32_t max_wave) : device_(dev), adm_(budget), max_wave_(max_wave ? max_wave : 256) {}
+  Server(int dev, uint64_t budget, uint32_t max_wave) : device_(dev), adm_(budget), max_wave_(max_wave ? max_wave : 256) {
+    // waves started with whatever is pending (see sched_loop); ZKGPU_SERVER_EAGER_WAVES overrides
+    const char* v = std::getenv("ZKGPU_SERVER_EAGER_WAVES");
+    if (v && *v) eager_waves_ = std::max(1, std::min(kStreams, std::atoi(v)));
+  }
 
   int start() {
     ZK_TRY("cudaSetDevice", cudaSetDevice(device_));
@@ -194,6 +199,7 @@ class Server {
  private:
   static constexpr int kStreams = 8;
   static constexpr int kEagerWaves = 2;
+  int eager_waves_ = kEagerWaves;
   // per MSM job in a wave's mailbox: window count, c, then the window sums
   static constexpr uint64_t kMsmSlotWords = 2 + 16 * (uint64_t)MSM_MAX_WINDOWS;
 
@@ -211,7 +217,7 @@ class Server {
         // launches and better overlap under load).
         cv_sched_.wait(lk, [&] {
           return stop_ || (adm_.pending() > 0 && waves_inflight_ < kStreams &&
-                           (waves_inflight_ < kEagerWaves || adm_.pending() >= max_wave_));
+                           (waves_inflight_ < eager_waves_ || adm_.pending() >= max_wave_));
         });
         if (stop_) return;
         const uint64_t gen = retired_gen_;
