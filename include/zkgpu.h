@@ -159,7 +159,10 @@ int zkgpu_ew_dev(int device, uint32_t op, uint64_t *d_out, const uint64_t *d_a, 
  * ZKGPU_EINVAL when t vanishes somewhere on the coset. */
 int zkgpu_divide_by_vanishing_dev(int device, uint64_t *d_ext, uint32_t log_n, uint32_t log_ext, const uint64_t g[4],
                                   const uint64_t omega_ext[4], void *stream);
-/* d_out_xyz receives the Jacobian sum (12 words, device memory) */
+/* d_out_xyz receives the Jacobian sum (12 words, device memory), normalised
+ * (Z = Montgomery one, or all zero for the identity); the call stays
+ * asynchronous on `stream` (its last, serial step runs on the host as a
+ * stream-ordered host function). */
 int zkgpu_msm_dev(int device, const uint64_t *d_scalars, const uint64_t *d_bases_xy, uint64_t n, uint64_t *d_out_xyz,
                   void *stream);
 /* d_out_xy[i] = k_i * base (affine, Fq Montgomery, (0, 0) for the identity),

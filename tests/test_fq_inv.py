@@ -1,0 +1,25 @@
+"""CPU: the MSM's branch-free binary Fq inversion (fq_inv.cuh, compiled for
+the host from the same source the kernels use) against Python bigints, on
+random values and the edges 1, 2, (q-1)/2, q-1."""
+import os
+import random
+import shutil
+import subprocess
+
+import pytest
+
+Q = 21888242871839275222246405745257275088696311157297823662689037894645226208583
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="needs g++")
+def test_binary_inversion_matches_bigint(tmp_path):
+    exe = tmp_path / "fq_inv_check"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-o", str(exe), os.path.join(HERE, "fq_inv_check.cpp")], check=True)
+    rng = random.Random(2024)
+    vals = [1, 2, 3, (Q - 1) // 2, Q - 2, Q - 1, 1 << 253, (1 << 254) % Q] + [rng.randrange(1, Q) for _ in range(3000)]
+    inp = "".join(f"{v:064x}\n" for v in vals)
+    out = subprocess.run([str(exe)], input=inp, capture_output=True, text=True, check=True).stdout.split()
+    assert len(out) == len(vals)
+    for v, r in zip(vals, out):
+        assert int(r, 16) == pow(v, -1, Q), hex(v)

@@ -1,7 +1,12 @@
 // msm.cu — Pippenger MSM kernels and orchestration (see msm.cuh).
 #include <algorithm>
 
+#include <mutex>
+#include <vector>
+
 #include "curve.cuh"
+#include "fq_inv.cuh"
+#include "host_field.hpp"
 #include "msm.cuh"
 #include "prof.cuh"
 #include "runtime.cuh"
@@ -167,9 +172,11 @@ __global__ void scan_add_kernel(uint32_t* out, uint32_t* cursor, const uint32_t*
 //   apply   : each task walks its chain back (2 products per sum) and
 //             finishes the additions (lambda, lambda^2, lambda (x1 - x3):
 //             3 products).
-// That is about 6 + 331 / (BA_K BA_G) + 3 / BA_K ~ 6.8 Fq products per
-// point addition (the XYZZ mixed addition costs 10), with every inversion
-// amortised over 512 additions and no serial block-wide step.  Equal x
+// That is about 6 + 3 / BA_K ~ 6.2 Fq products per point addition (the XYZZ
+// mixed addition costs 10) plus one inversion per 512 additions, done by
+// the branch-free binary algorithm of fq_inv.cuh (shifts and subtractions,
+// ~0.01 ms of latency against ~0.18 ms for a Fermat power), with no serial
+// block-wide step.  Equal x
 // (P = Q: doubling, denominator 2y; P = -Q: identity) and the identity
 // (x = 0: no BN254 point has x = 0, as 3 is not a square mod q) are handled
 // per sum.  A bucket reaching one point writes it to `fin`; after the last
@@ -181,25 +188,17 @@ constexpr uint32_t BA_G = 32;  // task products per inversion
 
 __device__ __forceinline__ void fq_one_rp(uint32_t r[8]) { set_one_rp<FqP>(r); }
 
-// a^(q-2) = a^-1 (a != 0), R' form, lazy in, canonical out; 4-bit fixed
-// windows: 254 squarings + 63 products + 14 for the table
-__device__ __noinline__ void fq_inv_rp_w4(uint32_t r[8], const uint32_t a[8]) {
-  uint32_t tab[16][8];
-  fq_one_rp(tab[0]);
-  cpy(tab[1], a);
-  for (int i = 2; i < 16; i++) qmul(tab[i], tab[i - 1], a);
-  const uint32_t e[8] = {FqP::P0 - 2u, FqP::P1, FqP::P2, FqP::P3, FqP::P4, FqP::P5, FqP::P6, FqP::P7};
-  uint32_t acc[8];
-  cpy(acc, tab[e[7] >> 28]);
-  for (int nib = 62; nib >= 0; nib--) {
-    qsqr(acc, acc);
-    qsqr(acc, acc);
-    qsqr(acc, acc);
-    qsqr(acc, acc);
-    const uint32_t d = (e[nib >> 3] >> (4 * (nib & 7))) & 15u;
-    if (d) qmul(acc, acc, tab[d]);
-  }
-  reduce_once<FqP>(r, acc);
+// a^-1 for a != 0 in R' form (x 2^260), lazy in, canonical out: the binary
+// inversion (fq_inv.cuh) of the representative a 2^260 gives a^-1 2^-260,
+// and one product with 2^780 mod q returns it to R' form.
+__device__ __forceinline__ void fq_inv_rp_bin(uint32_t r[8], const uint32_t a[8]) {
+  const uint32_t k780[8] = {0x3fe3a1a8u, 0x13e32478u, 0x6ad256c5u, 0xc59c2897u,
+                            0x3603f972u, 0xc5387239u, 0x8d1987f5u, 0x10f16dedu};
+  uint32_t c[8], t[8];
+  reduce_once<FqP>(c, a);
+  fq_inv_binary(t, c);
+  qmul(r, t, k780);
+  reduce_once<FqP>(r, r);
 }
 
 // the point at position pos of a round's input: round 0 gathers the signed
@@ -331,7 +330,7 @@ __global__ void __launch_bounds__(128) ba_invert_kernel(fe* tot, fe* tpre, const
       st_fe(tpre + i, acc);
     }
     uint32_t inv[8];
-    fq_inv_rp_w4(inv, acc);
+    fq_inv_rp_bin(inv, acc);
     for (uint32_t i = i1 - 1; i > i0; i--) {
       uint32_t p[8], it[8];
       ld_fe(p, tpre + i - 1);
@@ -560,23 +559,6 @@ __global__ void __launch_bounds__(256) msm_window_kernel(const fe* segres, fe* w
   }
 }
 
-// Horner over windows (high to low) and conversion to Jacobian.
-__global__ void msm_combine_kernel(const fe* winsum, uint32_t windows, uint32_t c, fe* out) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  xyzz_t acc, t;
-  ld_xyzz(acc, winsum + 4 * (uint64_t)(windows - 1));
-  for (int w = (int)windows - 2; w >= 0; w--) {
-    for (uint32_t k = 0; k < c; k++) xyzz_dbl(acc, acc);
-    ld_xyzz(t, winsum + 4 * (uint64_t)w);
-    xyzz_add(acc, t);
-  }
-  uint32_t j[24];
-  xyzz_to_jacobian(j, acc);
-  st_fe(out, j);
-  st_fe(out + 1, j + 8);
-  st_fe(out + 2, j + 16);
-}
-
 // bases (R form, as the API holds them) -> R' form for the curve arithmetic
 __global__ void msm_convert_bases_kernel(const fe* in, fe* out, uint64_t n) {
   const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
@@ -598,6 +580,55 @@ __global__ void zero_out_kernel(fe* out) {
 }
 
 namespace {
+// The Horner step over the window sums (sum_w 2^(c w) W_w, ~250 dependent
+// doublings) is serial: one GPU thread needs over a millisecond for it, the
+// host well under 0.1 ms.  The device-resident call keeps stream order and
+// asynchrony by running it as a host function on the stream: window sums to
+// a pinned slot, host_horner() on the stream, the normalised Jacobian result
+// back to the caller's device buffer.  Slots are per host thread and reused
+// round robin once the event of their last use has completed.
+struct HornerSlot {
+  uint64_t win[MSM_MAX_WINDOWS * 16];
+  uint64_t out[12];
+  uint32_t windows = 0, c = 0;
+  cudaEvent_t done = nullptr;
+};
+constexpr int kHornerSlots = 8;
+struct HornerRing {
+  HornerSlot* slots = nullptr;  // pinned, kHornerSlots entries
+  int next = 0;
+};
+thread_local HornerRing t_horner;
+
+void CUDART_CB host_horner(void* arg) {
+  HornerSlot* h = static_cast<HornerSlot*>(arg);
+  host::fq::msm_combine_windows(h->win, h->windows, h->c, h->out);
+}
+
+cudaError_t horner_on_host(const fe* d_winsum, uint32_t windows, uint32_t c, fe* d_out, cudaStream_t s) {
+  HornerRing& r = t_horner;
+  if (!r.slots) {
+    cudaError_t e = cudaMallocHost((void**)&r.slots, sizeof(HornerSlot) * kHornerSlots);
+    if (e != cudaSuccess) return e;
+    for (int i = 0; i < kHornerSlots; i++) {
+      new (&r.slots[i]) HornerSlot();
+      e = cudaEventCreateWithFlags(&r.slots[i].done, cudaEventDisableTiming);
+      if (e != cudaSuccess) return e;
+    }
+  }
+  HornerSlot* h = &r.slots[r.next];
+  r.next = (r.next + 1) % kHornerSlots;
+  cudaError_t e = cudaEventSynchronize(h->done);  // its last use has finished (normally long ago)
+  if (e != cudaSuccess) return e;
+  h->windows = windows;
+  h->c = c;
+  e = cudaMemcpyAsync(h->win, d_winsum, windows * 128ull, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaLaunchHostFunc(s, host_horner, h);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_out, h->out, 96, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaEventRecord(h->done, s);
+  return e;
+}
+
 // Buffer sizes of one MSM pass (msm_run_impl allocates exactly these;
 // msm_scratch_bytes reports them for admission).
 struct MsmLayout {
@@ -805,11 +836,8 @@ cudaError_t msm_run_impl(const fe* d_scalars, const fe* d_bases, uint64_t n, fe*
     }
     msm_window_kernel<<<W, 256, 0, s>>>(segres, winsum, B / L);
     nl += 2;
-    if (!wout) {
-      msm_combine_kernel<<<1, 32, 0, s>>>(winsum, W, (uint32_t)p.c, d_out);
-      nl++;
-    }
     e = cudaGetLastError();
+    if (!wout && e == cudaSuccess) e = horner_on_host(winsum, W, (uint32_t)p.c, d_out, s);
   }
   for (void* ptr : {(void*)counts, (void*)offsets, (void*)cursor, (void*)bsums, (void*)list, (void*)cnt,
                     (void*)cprev, (void*)np, (void*)joff[0], (void*)joff[1], (void*)fin, (void*)buf[0],

@@ -13,7 +13,8 @@
 //                 round from Montgomery's trick (batch-affine accumulation).
 //   4. reduce   : per window, sum_b b * B_b by segmented running sums
 //                 (segment results T_s + lo_s * S_s), then a block tree sum.
-//   5. combine  : Horner over windows, sum_w 2^(c w) W_w, as Jacobian.
+//   5. combine  : Horner over windows, sum_w 2^(c w) W_w, on the host (the
+//                 ~250 dependent doublings are serial), normalised Jacobian.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -36,7 +37,9 @@ MsmPlan make_msm_plan(uint64_t n, int c_override = 0, int device = -1);
 int tuned_msm_window(int device, int log_n);
 
 // Enqueue the MSM on `s`; d_out receives the Jacobian sum (X, Y, Z: 12 u64,
-// not normalised; identity = Z 0).  Scratch comes from the stream pool.
+// normalised to Z = one; all zero for the identity), the last step (Horner
+// over the windows) running as a host function on the stream.  Scratch
+// comes from the library pool.
 // Optional: stop before the last step and leave the per-window sums for the
 // host (host::fq::msm_combine_windows), which does the ~250 dependent
 // doublings of the Horner step far faster than one GPU thread.
