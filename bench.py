@@ -156,9 +156,10 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # reference arm: the CPU path on host cores
 # ---------------------------------------------------------------------------
-def cpu_lde_sample(k: int = 22, e: int = 2, seed: int = 5):
+def cpu_lde_sample(k: int = LOG_N, e: int = LOG_EXT - LOG_N, seed: int = 5):
     """halo2 CPU LDE (oracle restatement of best_fft/ifft/distribute_powers) on
-    a 2^k -> 2^(k+e) sample; returns (seconds, threads)."""
+    a 2^k -> 2^(k+e) input, the full benchmark size by default; returns
+    (seconds, threads)."""
     from oracle import pyoracle as O
     threads = os.cpu_count() or 1
     c = lde_constants(k, e)
@@ -174,8 +175,9 @@ def lde_work(k: int, e: int) -> float:
     return (2**k / 2) * k + 2**k + 2**k + (2 ** (k + e) / 2) * (k + e)
 
 
-def cpu_melem_s(t_sample: float, k: int = 22, e: int = 2) -> float:
-    # scale the sample's time to the full 2^24 -> 2^26 workload by algorithmic work
+def cpu_melem_s(t_sample: float, k: int = LOG_N, e: int = LOG_EXT - LOG_N) -> float:
+    # a smaller sample's time scales to the full 2^24 -> 2^26 workload by
+    # algorithmic work (the default sample is the full workload: factor 1)
     t_full = t_sample * lde_work(LOG_N, LOG_EXT - LOG_N) / lde_work(k, e)
     return (2**LOG_N) / t_full / 1e6
 
@@ -191,8 +193,8 @@ def run_reference(args, rank: int, world: int):
             ts.append(t)
     t = statistics.median(ts)
     v = cpu_melem_s(t)
-    sample = ("halo2 LDE 2^22 -> 2^24 per step (oracle port of best_fft/ifft/distribute_powers, OpenMP), "
-              "time scaled to 2^24 -> 2^26 by algorithmic work")
+    sample = ("one full halo2 LDE 2^24 -> 2^26 per step (oracle port of best_fft/ifft/distribute_powers, "
+              "OpenMP on all host threads)")
     line = {
         "impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "Melem/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t * 1e3, 3), "higher_is_better": True,
@@ -374,8 +376,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         t, threads = cpu_lde_sample()
         line["cpu_baseline"] = {"value": round(cpu_melem_s(t), 3), "unit": "Melem/s", "cores": threads,
                                 "kind": "port",
-                                "sample": "halo2 LDE 2^22 -> 2^24 once (oracle port, OpenMP on all host threads), "
-                                          "time scaled to 2^24 -> 2^26 by algorithmic work"}
+                                "sample": "one full halo2 LDE 2^24 -> 2^26 (oracle port, OpenMP on all host threads)"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     group.barrier()

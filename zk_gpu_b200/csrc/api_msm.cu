@@ -26,15 +26,15 @@ int msm_host(int device, const uint64_t* scalars, const uint64_t* bases_xy, uint
   cudaError_t e = zk::dmalloc((void**)&ds, n * 32, s);
   if (e == cudaSuccess) e = zk::dmalloc((void**)&db, n * 64, s);
   if (e == cudaSuccess) e = zk::dmalloc((void**)&dwin, zk::MSM_MAX_WINDOWS * 128, s);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(ds, scalars, n * 32, cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(db, bases_xy, n * 64, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = zk::h2d_copy(ds, scalars, n * 32, s);
+  if (e == cudaSuccess) e = zk::h2d_copy(db, bases_xy, n * 64, s);
   uint64_t nl = 0;
   zk::MsmWindowsOut wo;
   wo.d_winsum = dwin;
   if (e == cudaSuccess) e = zk::msm_run(ds, db, n, nullptr, s, 0, &nl, &wo);
   zk::count_launches(nl);
   if (e == cudaSuccess && wo.windows > zk::MSM_MAX_WINDOWS) e = cudaErrorInvalidValue;
-  if (e == cudaSuccess) e = cudaMemcpyAsync(win, dwin, wo.windows * 128ull, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = zk::d2h_copy(win, dwin, wo.windows * 128ull, s);
   if (ds) cudaFreeAsync(ds, s);
   if (db) cudaFreeAsync(db, s);
   if (dwin) cudaFreeAsync(dwin, s);

@@ -61,10 +61,10 @@ int ntt_host(int device, uint64_t* a, uint32_t log_n, const uint64_t* omega, con
   const size_t bytes = ((size_t)1 << log_n) * sizeof(fe);
   fe* d = nullptr;
   ZK_TRY("zk::dmalloc(ntt data)", zk::dmalloc((void**)&d, bytes, s));
-  cudaError_t e = cudaMemcpyAsync(d, a, bytes, cudaMemcpyHostToDevice, s);
+  cudaError_t e = zk::h2d_copy(d, a, bytes, s);
   if (e == cudaSuccess) {
     st = ntt_device(device, d, log_n, load_fr(omega), coset, post, s);
-    if (st == ZKGPU_OK) e = cudaMemcpyAsync(a, d, bytes, cudaMemcpyDeviceToHost, s);
+    if (st == ZKGPU_OK) e = zk::d2h_copy(a, d, bytes, s);
   }
   cudaFreeAsync(d, s);
   cudaError_t e2 = cudaStreamSynchronize(s);
@@ -249,11 +249,11 @@ extern "C" int zkgpu_lagrange_to_extended(int device, const uint64_t* values, ui
     cudaFreeAsync(d_in, s);
     return zk::status_of("zk::dmalloc(lde ext)", e);
   }
-  e = cudaMemcpyAsync(d_in, values, n * sizeof(fe), cudaMemcpyHostToDevice, s);
+  e = zk::h2d_copy(d_in, values, n * sizeof(fe), s);
   if (e == cudaSuccess) {
     st = lde_device(device, d_in, log_n, d_ext, log_ext, load_fr(omega_inv), load_fr(divisor), load_fr(g),
                     load_fr(omega_ext), s);
-    if (st == ZKGPU_OK) e = cudaMemcpyAsync(ext, d_ext, N * sizeof(fe), cudaMemcpyDeviceToHost, s);
+    if (st == ZKGPU_OK) e = zk::d2h_copy(ext, d_ext, N * sizeof(fe), s);
   }
   cudaFreeAsync(d_in, s);
   cudaFreeAsync(d_ext, s);
@@ -318,11 +318,11 @@ extern "C" int zkgpu_extended_to_coeff(int device, const uint64_t* ext, uint32_t
     cudaFreeAsync(d_ext, s);
     return zk::status_of("zk::dmalloc(ext_to_coeff out)", e);
   }
-  e = cudaMemcpyAsync(d_ext, ext, N * sizeof(fe), cudaMemcpyHostToDevice, s);
+  e = zk::h2d_copy(d_ext, ext, N * sizeof(fe), s);
   if (e == cudaSuccess) {
     st = ext_to_coeff_device(device, d_ext, log_ext, load_fr(omega_ext_inv), load_fr(ext_divisor), load_fr(g_inv),
                              d_out, m, s);
-    if (st == ZKGPU_OK) e = cudaMemcpyAsync(out, d_out, m * sizeof(fe), cudaMemcpyDeviceToHost, s);
+    if (st == ZKGPU_OK) e = zk::d2h_copy(out, d_out, m * sizeof(fe), s);
   }
   cudaFreeAsync(d_ext, s);
   cudaFreeAsync(d_out, s);
@@ -380,8 +380,8 @@ extern "C" int zkgpu_field_op(int device, int op, int fid, const uint64_t* a, co
   ZK_TRY("cudaMallocAsync", zk::dmalloc((void**)&da, bytes, s));
   ZK_TRY("cudaMallocAsync", zk::dmalloc((void**)&db, bytes, s));
   ZK_TRY("cudaMallocAsync", zk::dmalloc((void**)&dout, bytes, s));
-  cudaMemcpyAsync(da, a, bytes, cudaMemcpyHostToDevice, s);
-  cudaMemcpyAsync(db, b, bytes, cudaMemcpyHostToDevice, s);
+  zk::h2d_copy(da, a, bytes, s);
+  zk::h2d_copy(db, b, bytes, s);
   const unsigned grid = (unsigned)((n + 255) / 256);
   if (fid == 0)
     field_op_kernel<zk::FrP><<<grid, 256, 0, s>>>(op, da, db, dout, n);
@@ -389,7 +389,7 @@ extern "C" int zkgpu_field_op(int device, int op, int fid, const uint64_t* a, co
     field_op_kernel<zk::FqP><<<grid, 256, 0, s>>>(op, da, db, dout, n);
   zk::count_launches(1);
   cudaError_t e = cudaGetLastError();
-  if (e == cudaSuccess) e = cudaMemcpyAsync(out, dout, bytes, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = zk::d2h_copy(out, dout, bytes, s);
   cudaFreeAsync(da, s);
   cudaFreeAsync(db, s);
   cudaFreeAsync(dout, s);

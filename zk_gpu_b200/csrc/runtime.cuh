@@ -32,6 +32,15 @@ int bind_device(int device, cudaStream_t* stream);
 cudaError_t dmalloc(void** ptr, size_t bytes, cudaStream_t s);
 // Return the library pool's cached, unused memory on `device` to the system.
 cudaError_t trim_pool(int device);
+// Copies for the host-buffer entry points, enqueued on `s`.  Pinned host
+// memory is copied directly; pageable memory goes through a per-thread ring
+// of pinned chunks (staging.cu).  h2d_copy returns once the source is no
+// longer needed (pageable) or the copy is enqueued (pinned); d2h_copy on
+// pageable memory returns with the data in `dst`, on pinned memory once the
+// copy is enqueued.
+bool host_pinned(const void* p);
+cudaError_t h2d_copy(void* dst, const void* src, size_t n, cudaStream_t s);
+cudaError_t d2h_copy(void* dst, const void* src, size_t n, cudaStream_t s);
 template <class T>
 inline cudaError_t dmalloc(T** ptr, size_t bytes, cudaStream_t s) {
   return dmalloc(reinterpret_cast<void**>(ptr), bytes, s);
