@@ -54,6 +54,10 @@ struct JobRec {
   clk::time_point t_submit, t_done;
   int status = -1;  // -1 in progress
   uint64_t* msm_out = nullptr;  // slot in the wave's pinned mailbox
+  cudaEvent_t done_ev = nullptr;  // after this job's result copy (its completion on the GPU side)
+  bool retired = false;           // its wave retired (memory released)
+  bool taken = false;             // a waiter collected the result
+  bool early_failed = false;      // its result is not good: reported at retirement
 };
 
 struct Wave {
@@ -173,9 +177,15 @@ class Server {
       cv_done_.wait(lk, done);
     else if (!cv_done_.wait_for(lk, std::chrono::milliseconds(timeout_ms), done))
       return ZKGPU_ETIMEOUT;
+    if (r->taken) return ZKGPU_EINVAL;  // already waited for
     if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
     const int st = r->status;
-    jobs_.erase(it);
+    // a job can complete before its wave retires; the wave still reads the
+    // record until then, so the retirement erases it
+    if (r->retired)
+      jobs_.erase(it);
+    else
+      r->taken = true;
     return st;
   }
 
@@ -198,7 +208,7 @@ class Server {
 
  private:
   static constexpr int kStreams = 8;
-  static constexpr int kEagerWaves = 2;
+  static constexpr int kEagerWaves = kStreams;
   int eager_waves_ = kEagerWaves;
   // per MSM job in a wave's mailbox: window count, c, then the window sums
   static constexpr uint64_t kMsmSlotWords = 2 + 16 * (uint64_t)MSM_MAX_WINDOWS;
@@ -358,6 +368,7 @@ class Server {
             ok(cudaMemcpyAsync(r->msm_out + 2, dwin + (size_t)k * wo.windows * 4, wo.windows * 128ull,
                                cudaMemcpyDeviceToHost, w.s_msm));
           }
+          for (JobRec* r : grp) record_done(r, w.s_msm);
         }
       }
       frees_msm.push_back(ds);
@@ -384,6 +395,7 @@ class Server {
             r->msm_out[0] = wo.windows;
             r->msm_out[1] = wo.c;
             ok(cudaMemcpyAsync(r->msm_out + 2, dwin, wo.windows * 128ull, cudaMemcpyDeviceToHost, w.s_msm));
+            record_done(r, w.s_msm);
           }
         }
         frees_msm.push_back(ds);
@@ -491,10 +503,19 @@ class Server {
       }
       frees_ntt.push_back(dp);
       frees_ntt.push_back(dc);
+      // results back smallest first, each job complete when its own copy is
+      // (a small job does not wait for a large one's download)
+      auto out_bytes = [](const JobRec* r) {
+        const zkgpu_job& j = r->job;
+        return ((size_t)1 << (j.kind == ZKGPU_KIND_LDE ? j.log_ext : j.log_n)) * 32;
+      };
+      std::stable_sort(ntt_outputs.begin(), ntt_outputs.end(),
+                       [&](const std::pair<JobRec*, fe*>& x, const std::pair<JobRec*, fe*>& y) {
+                         return out_bytes(x.first) < out_bytes(y.first);
+                       });
       for (auto& o : ntt_outputs) {
-        const zkgpu_job& j = o.first->job;
-        const uint32_t L = j.kind == ZKGPU_KIND_LDE ? j.log_ext : j.log_n;
-        ok(cudaMemcpyAsync(j.output, o.second, ((size_t)1 << L) * 32, cudaMemcpyDeviceToHost, w.s_ntt));
+        ok(cudaMemcpyAsync(o.first->job.output, o.second, out_bytes(o.first), cudaMemcpyDeviceToHost, w.s_ntt));
+        record_done(o.first, w.s_ntt);
       }
     }
     for (const NttItem& it : items) {
@@ -511,51 +532,116 @@ class Server {
     if (e != cudaSuccess) w.status = status_of("server wave", e);
   }
 
+  // per-job completion event on the stream that produced the job's result
+  static void record_done(JobRec* r, cudaStream_t s) {
+    if (!r->done_ev && cudaEventCreateWithFlags(&r->done_ev, cudaEventDisableTiming) != cudaSuccess) {
+      r->done_ev = nullptr;  // fall back to the wave's completion
+      return;
+    }
+    cudaEventRecord(r->done_ev, s);
+  }
+
+  // finish one job on the host (MSM: Horner step into the caller's output)
+  // and wake its waiter; the wave's memory is released when the wave retires
+  void finish_job(JobRec* r, int st) {
+    if (st == ZKGPU_OK && r->job.kind == ZKGPU_KIND_MSM && r->msm_out) {
+      uint64_t out[12];
+      host::fq::msm_combine_windows(r->msm_out + 2, (uint32_t)r->msm_out[0], (uint32_t)r->msm_out[1], out);
+      std::memcpy(r->job.output, out, 96);
+    }
+    const auto now = clk::now();
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      r->status = st;
+      r->t_done = now;
+      if (st == ZKGPU_OK)
+        completed_++;
+      else
+        failed_++;
+    }
+    cv_done_.notify_all();
+  }
+
+  // Completion: jobs of every wave in flight finish one by one as their own
+  // result copies land; waves retire in launch order once both their streams
+  // are done, which releases their memory to the budget.
   void comp_loop() {
     cudaSetDevice(device_);
     for (;;) {
-      std::unique_ptr<Wave> w;
+      std::vector<Wave*> live;
       {
         std::unique_lock<std::mutex> lk(mu_);
-        cv_comp_.wait(lk, [&] { return !inflight_.empty() || (stop_ && inflight_.empty()); });
-        if (inflight_.empty()) return;
-        w = std::move(inflight_.front());
-        inflight_.pop_front();
+        cv_comp_.wait(lk, [&] { return !inflight_.empty() || stop_; });
+        if (inflight_.empty()) return;  // stop_ and nothing left
+        for (auto& w : inflight_) live.push_back(w.get());  // only this thread pops: pointers stay valid
       }
-      cudaError_t e1 = cudaEventSynchronize(w->ev_ntt);
-      cudaError_t e2 = cudaEventSynchronize(w->ev_msm);
-      int st = w->status;
-      if (st == ZKGPU_OK && (e1 != cudaSuccess || e2 != cudaSuccess))
-        st = status_of("server wave sync", e1 != cudaSuccess ? e1 : e2);
-      if (st == ZKGPU_OK && (uint32_t)w->mailbox[0]) st = ZKGPU_ETIMEOUT;
-      const auto now = clk::now();
-      for (JobRec* r : w->jobs)
-        if (st == ZKGPU_OK && r->job.kind == ZKGPU_KIND_MSM && r->msm_out) {
-          uint64_t out[12];
-          host::fq::msm_combine_windows(r->msm_out + 2, (uint32_t)r->msm_out[0], (uint32_t)r->msm_out[1], out);
-          std::memcpy(r->job.output, out, 96);
-        }
-      cudaEventDestroy(w->ev_ntt);
-      cudaEventDestroy(w->ev_msm);
-      {
-        std::lock_guard<std::mutex> lk(mu_);
+      bool progressed = false;
+      for (Wave* w : live) {
+        if (w->status != ZKGPU_OK) continue;
         for (JobRec* r : w->jobs) {
-          r->status = st;
-          r->t_done = now;
-          adm_.release(r->bytes);
-          if (st == ZKGPU_OK)
-            completed_++;
-          else
-            failed_++;
+          if (r->status >= 0 || !r->done_ev || r->early_failed) continue;
+          const cudaError_t q = cudaEventQuery(r->done_ev);
+          if (q == cudaErrorNotReady) continue;
+          progressed = true;
+          // an NTT / LDE result is good only if the batch kernel met every
+          // wait: its error flag was copied before any of the wave's results
+          if (q != cudaSuccess || (r->job.kind != ZKGPU_KIND_MSM && (uint32_t)w->mailbox[0])) {
+            r->early_failed = true;  // reported when the wave retires
+            continue;
+          }
+          finish_job(r, ZKGPU_OK);
         }
-        adm_.release(w->extra_bytes);
-        inflight_jobs_ -= w->jobs.size();
-        waves_inflight_--;
-        retired_gen_++;
       }
-      cv_done_.notify_all();
-      cv_sched_.notify_all();
+      for (;;) {  // retire finished waves in order
+        Wave* w;
+        {
+          std::lock_guard<std::mutex> lk(mu_);
+          if (inflight_.empty()) break;
+          w = inflight_.front().get();
+        }
+        const cudaError_t q1 = cudaEventQuery(w->ev_ntt), q2 = cudaEventQuery(w->ev_msm);
+        if (q1 == cudaErrorNotReady || q2 == cudaErrorNotReady) break;
+        retire(w, q1, q2);
+        progressed = true;
+      }
+      if (!progressed) {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_comp_.wait_for(lk, std::chrono::microseconds(50));
+      }
     }
+  }
+
+  void retire(Wave* w, cudaError_t e1, cudaError_t e2) {
+    int st = w->status;
+    if (st == ZKGPU_OK && (e1 != cudaSuccess || e2 != cudaSuccess))
+      st = status_of("server wave sync", e1 != cudaSuccess ? e1 : e2);
+    if (st == ZKGPU_OK && (uint32_t)w->mailbox[0]) st = ZKGPU_ETIMEOUT;
+    for (JobRec* r : w->jobs)
+      if (r->status < 0) finish_job(r, st);
+    for (JobRec* r : w->jobs)
+      if (r->done_ev) {
+        cudaEventDestroy(r->done_ev);
+        r->done_ev = nullptr;
+      }
+    cudaEventDestroy(w->ev_ntt);
+    cudaEventDestroy(w->ev_msm);
+    std::unique_ptr<Wave> keep;  // destroyed after the lock: it releases table references
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      for (JobRec* r : w->jobs) {
+        adm_.release(r->bytes);
+        r->retired = true;
+        if (r->taken) jobs_.erase(r->ticket);
+      }
+      adm_.release(w->extra_bytes);
+      inflight_jobs_ -= w->jobs.size();
+      waves_inflight_--;
+      retired_gen_++;
+      keep = std::move(inflight_.front());
+      inflight_.pop_front();
+    }
+    cv_done_.notify_all();
+    cv_sched_.notify_all();
   }
 
   int device_;
