@@ -108,3 +108,99 @@ __host__ __device__ inline void fq_inv_binary(uint32_t r[8], const uint32_t a[8]
 }
 
 }  // namespace zk
+
+#ifdef __CUDACC__
+namespace zk {
+
+// The same algorithm for device code with every multi-word add / subtract a
+// single carry chain (sub.cc / subc, add.cc / addc) inside one asm statement:
+// a step's dependent path is a few short chains instead of emulated 64-bit
+// borrows, which cuts the inversion's latency several times.  Tested through
+// the MSM tests (every result bit-exact) and against fq_inv_binary's host
+// check by construction (identical step semantics).
+#define ZK_INV_SUB8(d, a, b, br)                                                                        \
+  asm("sub.cc.u32  %0, %9, %17;\n\tsubc.cc.u32 %1, %10, %18;\n\tsubc.cc.u32 %2, %11, %19;\n\t"          \
+      "subc.cc.u32 %3, %12, %20;\n\tsubc.cc.u32 %4, %13, %21;\n\tsubc.cc.u32 %5, %14, %22;\n\t"         \
+      "subc.cc.u32 %6, %15, %23;\n\tsubc.cc.u32 %7, %16, %24;\n\tsubc.u32 %8, 0, 0;"                     \
+      : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]), \
+        "=r"(br)                                                                                         \
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]),          \
+        "r"(b[0]), "r"(b[1]), "r"(b[2]), "r"(b[3]), "r"(b[4]), "r"(b[5]), "r"(b[6]), "r"(b[7]))
+// d += b (8 words, carry out dropped)
+#define ZK_INV_ADD8(d, b)                                                                               \
+  asm("add.cc.u32  %0, %0, %8;\n\taddc.cc.u32 %1, %1, %9;\n\taddc.cc.u32 %2, %2, %10;\n\t"              \
+      "addc.cc.u32 %3, %3, %11;\n\taddc.cc.u32 %4, %4, %12;\n\taddc.cc.u32 %5, %5, %13;\n\t"            \
+      "addc.cc.u32 %6, %6, %14;\n\taddc.u32 %7, %7, %15;"                                               \
+      : "+r"(d[0]), "+r"(d[1]), "+r"(d[2]), "+r"(d[3]), "+r"(d[4]), "+r"(d[5]), "+r"(d[6]), "+r"(d[7])  \
+      : "r"(b[0]), "r"(b[1]), "r"(b[2]), "r"(b[3]), "r"(b[4]), "r"(b[5]), "r"(b[6]), "r"(b[7]))
+
+__device__ __forceinline__ void fq_inv_binary_dev(uint32_t r[8], const uint32_t a[8]) {
+  const uint32_t q[8] = {0xd87cfd47u, 0x3c208c16u, 0x6871ca8du, 0x97816a91u,
+                         0x8181585du, 0xb85045b6u, 0xe131a029u, 0x30644e72u};
+  uint32_t u[8], v[8], x1[8], x2[8];
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    u[i] = a[i];
+    v[i] = q[i];
+    x1[i] = i == 0 ? 1u : 0u;
+    x2[i] = 0u;
+  }
+#pragma unroll 1
+  for (int step = 0; step < 508; step++) {
+    const uint32_t m_odd = 0u - (u[0] & 1u);
+    uint32_t d[8], m_lt;
+    ZK_INV_SUB8(d, u, v, m_lt);  // m_lt: all ones iff u < v
+    const uint32_t m_swap = m_odd & m_lt;
+    // |u - v| = (d ^ m) - m
+    uint32_t ad[8], neg1[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      ad[i] = d[i] ^ m_lt;
+      neg1[i] = i == 0 ? (m_lt & 1u) : 0u;
+    }
+    ZK_INV_ADD8(ad, neg1);
+    // x1 - x2 and x2 - x1, mod q
+    uint32_t dx[8], rx[8], b1, b2;
+    ZK_INV_SUB8(dx, x1, x2, b1);
+    ZK_INV_SUB8(rx, x2, x1, b2);
+    uint32_t q1[8], q2[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      q1[i] = q[i] & b1;
+      q2[i] = q[i] & b2;
+    }
+    ZK_INV_ADD8(dx, q1);
+    ZK_INV_ADD8(rx, q2);
+    uint32_t nu[8], nx[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const uint32_t vi = (u[i] & m_swap) | (v[i] & ~m_swap);
+      const uint32_t x2i = (x1[i] & m_swap) | (x2[i] & ~m_swap);
+      const uint32_t dxi = (rx[i] & m_lt) | (dx[i] & ~m_lt);
+      nu[i] = (ad[i] & m_odd) | (u[i] & ~m_odd);
+      nx[i] = (dxi & m_odd) | (x1[i] & ~m_odd);
+      v[i] = vi;
+      x2[i] = x2i;
+    }
+    // u /= 2; x1 = x1 / 2 mod q
+    const uint32_t m_xodd = 0u - (nx[0] & 1u);
+    uint32_t qx[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) qx[i] = q[i] & m_xodd;
+    ZK_INV_ADD8(nx, qx);  // x + q < 2^255: no carry out
+#pragma unroll
+    for (int i = 0; i < 7; i++) {
+      u[i] = __funnelshift_r(nu[i], nu[i + 1], 1);
+      x1[i] = __funnelshift_r(nx[i], nx[i + 1], 1);
+    }
+    u[7] = nu[7] >> 1;
+    x1[7] = nx[7] >> 1;
+  }
+#pragma unroll
+  for (int i = 0; i < 8; i++) r[i] = x2[i];
+}
+#undef ZK_INV_SUB8
+#undef ZK_INV_ADD8
+
+}  // namespace zk
+#endif

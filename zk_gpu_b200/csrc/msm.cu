@@ -196,7 +196,7 @@ __device__ __forceinline__ void fq_inv_rp_bin(uint32_t r[8], const uint32_t a[8]
                             0x3603f972u, 0xc5387239u, 0x8d1987f5u, 0x10f16dedu};
   uint32_t c[8], t[8];
   reduce_once<FqP>(c, a);
-  fq_inv_binary(t, c);
+  fq_inv_binary_dev(t, c);
   qmul(r, t, k780);
   reduce_once<FqP>(r, r);
 }
@@ -314,13 +314,18 @@ __global__ void __launch_bounds__(256) ba_prefix_kernel(const fe* src, const uin
   }
 }
 
-// invert: thread s turns tot[s G .. s G + G) into their inverses
-__global__ void __launch_bounds__(128) ba_invert_kernel(fe* tot, fe* tpre, const uint32_t* joff, uint32_t T) {
+// invert: thread s turns tot[s G .. s G + G) into their inverses.  The
+// group length G follows the round's size: up to BA_G task products per
+// inversion when there are many, down to one when a round is small, so that
+// the round's latency is one inversion plus a short chain.
+__global__ void __launch_bounds__(128) ba_invert_kernel(fe* tot, fe* tpre, const uint32_t* joff, uint32_t T,
+                                                        uint32_t fill) {
   const uint32_t J = joff[T];
   const uint32_t tasks = (J + BA_K - 1) / BA_K;
-  const uint32_t groups = (tasks + BA_G - 1) / BA_G;
+  const uint32_t G = max(1u, min(BA_G, tasks / fill));
+  const uint32_t groups = (tasks + G - 1) / G;
   for (uint32_t sgi = blockIdx.x * blockDim.x + threadIdx.x; sgi < groups; sgi += gridDim.x * blockDim.x) {
-    const uint32_t i0 = sgi * BA_G, i1 = min(i0 + BA_G, tasks);
+    const uint32_t i0 = sgi * G, i1 = min(i0 + G, tasks);
     uint32_t acc[8], v[8];
     ld_fe(acc, tot + i0);
     st_fe(tpre + i0, acc);
@@ -800,14 +805,19 @@ cudaError_t msm_run_impl(const fe* d_scalars, const fe* d_bases, uint64_t n, fe*
         scan_block_kernel<<<nblk, 1024, 0, s>>>(np, jo, bsums, T);
         scan_sums_kernel<<<1, 1024, 0, s>>>(bsums, nblk, jo + T);
         scan_add_kernel<<<nblk, 1024, 0, s>>>(jo, cursor, bsums, T);
-        const uint64_t tasks = (jb + BA_K - 1) / BA_K, groups = (tasks + BA_G - 1) / BA_G;
+        // inversion threads: enough to fill the GPU (fill groups), each group
+        // at most BA_G task products; the grid covers the one-task groups of
+        // a small round
+        const uint64_t tasks = (jb + BA_K - 1) / BA_K;
+        const uint32_t fill = (uint32_t)sms * 32;
         const unsigned gt = (unsigned)std::min<uint64_t>((tasks + 255) / 256, (uint64_t)sms * 6);
+        const uint64_t groups = tasks < fill ? tasks : std::max<uint64_t>(2ull * fill, tasks / BA_G + 1);
         const unsigned gi = (unsigned)std::min<uint64_t>((groups + 127) / 128, (uint64_t)sms * 8);
         if (first)
           ba_prefix_kernel<true><<<gt, 256, 0, s>>>(src, list, in_off, cprev, jo, np, T, pre, tot);
         else
           ba_prefix_kernel<false><<<gt, 256, 0, s>>>(src, list, in_off, cprev, jo, np, T, pre, tot);
-        ba_invert_kernel<<<gi, 128, 0, s>>>(tot, tpre, jo, T);
+        ba_invert_kernel<<<gi, 128, 0, s>>>(tot, tpre, jo, T, fill);
         if (first)
           ba_apply_kernel<true><<<gt, 256, 0, s>>>(src, list, in_off, cprev, jo, np, T, pre, tot, dst, fin, cnt);
         else
