@@ -289,14 +289,23 @@ __global__ void ba_jobs_kernel(const uint32_t* cnt, uint32_t* cprev, uint32_t* n
 }
 
 // prefix: task t covers jobs [t K, t K + K) of the round (J = joff[T])
+// pair sums per task in a round of J sums: BA_K when the round fills the GPU
+// with tasks, fewer (down to one) in small rounds, whose latency is then one
+// short chain instead of BA_K dependent gathers and products
+__device__ __forceinline__ uint32_t ba_task_len(uint32_t J, uint32_t fill_k) {
+  return max(1u, min(BA_K, J / fill_k));
+}
+
 template <bool FIRST>
 __global__ void __launch_bounds__(256) ba_prefix_kernel(const fe* src, const uint32_t* list, const uint32_t* in_off,
                                                         const uint32_t* cprev, const uint32_t* joff,
-                                                        const uint32_t* np, uint32_t T, fe* pre, fe* tot) {
+                                                        const uint32_t* np, uint32_t T, fe* pre, fe* tot,
+                                                        uint32_t fill_k) {
   const uint32_t J = joff[T];
-  const uint32_t tasks = (J + BA_K - 1) / BA_K;
+  const uint32_t K = ba_task_len(J, fill_k);
+  const uint32_t tasks = (J + K - 1) / K;
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < tasks; t += gridDim.x * blockDim.x) {
-    const uint32_t q0 = t * BA_K, q1 = min(q0 + BA_K, J);
+    const uint32_t q0 = t * K, q1 = min(q0 + K, J);
     uint32_t b = ba_bucket_of(joff, T, q0);
     uint32_t acc[8];
     for (uint32_t q = q0; q < q1; q++) {
@@ -319,9 +328,10 @@ __global__ void __launch_bounds__(256) ba_prefix_kernel(const fe* src, const uin
 // inversion when there are many, down to one when a round is small, so that
 // the round's latency is one inversion plus a short chain.
 __global__ void __launch_bounds__(128) ba_invert_kernel(fe* tot, fe* tpre, const uint32_t* joff, uint32_t T,
-                                                        uint32_t fill) {
+                                                        uint32_t fill, uint32_t fill_k) {
   const uint32_t J = joff[T];
-  const uint32_t tasks = (J + BA_K - 1) / BA_K;
+  const uint32_t K = ba_task_len(J, fill_k);
+  const uint32_t tasks = (J + K - 1) / K;
   const uint32_t G = max(1u, min(BA_G, tasks / fill));
   const uint32_t groups = (tasks + G - 1) / G;
   for (uint32_t sgi = blockIdx.x * blockDim.x + threadIdx.x; sgi < groups; sgi += gridDim.x * blockDim.x) {
@@ -353,11 +363,12 @@ template <bool FIRST>
 __global__ void __launch_bounds__(256) ba_apply_kernel(const fe* src, const uint32_t* list, const uint32_t* in_off,
                                                        const uint32_t* cprev, const uint32_t* joff,
                                                        const uint32_t* np, uint32_t T, const fe* pre, const fe* tot,
-                                                       fe* dst, fe* fin, uint32_t* cnt) {
+                                                       fe* dst, fe* fin, uint32_t* cnt, uint32_t fill_k) {
   const uint32_t J = joff[T];
-  const uint32_t tasks = (J + BA_K - 1) / BA_K;
+  const uint32_t K = ba_task_len(J, fill_k);
+  const uint32_t tasks = (J + K - 1) / K;
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < tasks; t += gridDim.x * blockDim.x) {
-    const uint32_t q0 = t * BA_K, q1 = min(q0 + BA_K, J);
+    const uint32_t q0 = t * K, q1 = min(q0 + K, J);
     uint32_t inv_run[8];
     ld_fe(inv_run, tot + t);
     uint32_t b = ba_bucket_of(joff, T, q1 - 1);
@@ -634,6 +645,12 @@ cudaError_t horner_on_host(const fe* d_winsum, uint32_t windows, uint32_t c, fe*
   return e;
 }
 
+// tasks of a round of at most jb pair sums (ba_task_len: K = clamp(J / fill_k, 1, BA_K))
+uint64_t ba_tasks_bound(uint64_t jb, uint64_t fill_k) {
+  return std::max<uint64_t>(2 * fill_k, jb / BA_K + 1);
+}
+constexpr uint32_t kFillK = 148 * 64;  // task threads that fill a B200 (148 SMs) at 64 per SM
+
 // Buffer sizes of one MSM pass (msm_run_impl allocates exactly these;
 // msm_scratch_bytes reports them for admission).
 struct MsmLayout {
@@ -684,7 +701,7 @@ MsmLayout msm_layout(uint64_t n, uint32_t jobs, int c_override, int device = -1)
   l.rounds = lg > 3 ? lg - 2 : 1;
   l.jb[0] = l.E / 2 + l.T;
   l.jb[1] = l.jb[0] / 2 + l.T;
-  l.tasks0 = (l.jb[0] + BA_K - 1) / BA_K;
+  l.tasks0 = ba_tasks_bound(l.jb[0], kFillK);
   uint64_t jlast = l.jb[0];
   for (uint32_t r = 1; r < l.rounds; r++) jlast = jlast / 2 + l.T;
   l.chunks = l.T + jlast / BA_TS + 1;  // bound on sum_b max(1, ceil(cnt_b / BA_TS))
@@ -767,6 +784,7 @@ cudaError_t msm_run_impl(const fe* d_scalars, const fe* d_bases, uint64_t n, fe*
   if (e == cudaSuccess) {
     const double nd = (double)n;
     const int sms = sm_count();
+    const uint32_t fill_k = kFillK;  // matches the task buffers' bound (layout)
     cudaMemsetAsync(counts, 0, T * 4ull, s);
     const unsigned g = (unsigned)((n + 255) / 256);
     const unsigned gb = (T + 255) / 256;
@@ -808,20 +826,22 @@ cudaError_t msm_run_impl(const fe* d_scalars, const fe* d_bases, uint64_t n, fe*
         // inversion threads: enough to fill the GPU (fill groups), each group
         // at most BA_G task products; the grid covers the one-task groups of
         // a small round
-        const uint64_t tasks = (jb + BA_K - 1) / BA_K;
+        const uint64_t tasks = ba_tasks_bound(jb, fill_k);
         const uint32_t fill = (uint32_t)sms * 32;
         const unsigned gt = (unsigned)std::min<uint64_t>((tasks + 255) / 256, (uint64_t)sms * 6);
         const uint64_t groups = tasks < fill ? tasks : std::max<uint64_t>(2ull * fill, tasks / BA_G + 1);
         const unsigned gi = (unsigned)std::min<uint64_t>((groups + 127) / 128, (uint64_t)sms * 8);
         if (first)
-          ba_prefix_kernel<true><<<gt, 256, 0, s>>>(src, list, in_off, cprev, jo, np, T, pre, tot);
+          ba_prefix_kernel<true><<<gt, 256, 0, s>>>(src, list, in_off, cprev, jo, np, T, pre, tot, fill_k);
         else
-          ba_prefix_kernel<false><<<gt, 256, 0, s>>>(src, list, in_off, cprev, jo, np, T, pre, tot);
-        ba_invert_kernel<<<gi, 128, 0, s>>>(tot, tpre, jo, T, fill);
+          ba_prefix_kernel<false><<<gt, 256, 0, s>>>(src, list, in_off, cprev, jo, np, T, pre, tot, fill_k);
+        ba_invert_kernel<<<gi, 128, 0, s>>>(tot, tpre, jo, T, fill, fill_k);
         if (first)
-          ba_apply_kernel<true><<<gt, 256, 0, s>>>(src, list, in_off, cprev, jo, np, T, pre, tot, dst, fin, cnt);
+          ba_apply_kernel<true><<<gt, 256, 0, s>>>(src, list, in_off, cprev, jo, np, T, pre, tot, dst, fin, cnt,
+                                                   fill_k);
         else
-          ba_apply_kernel<false><<<gt, 256, 0, s>>>(src, list, in_off, cprev, jo, np, T, pre, tot, dst, fin, cnt);
+          ba_apply_kernel<false><<<gt, 256, 0, s>>>(src, list, in_off, cprev, jo, np, T, pre, tot, dst, fin, cnt,
+                                                    fill_k);
         nl += 7;
         jb = jb / 2 + T;
       }
