@@ -578,7 +578,8 @@ def serving_trace(njobs: int, seed: int = 99):
     return out
 
 
-def bench_serving(zk, torch, dev: int, njobs: int = 1000, rate: float = 2000.0, wave_jobs: int = 64):
+def bench_serving(zk, torch, dev: int, njobs: int = 1000, rate: float = 2000.0, wave_jobs: int = 64,
+                  hbm_budget: int = 150 * 10**9):
     """Serving loop (continuous batching) vs one call per job on the same GPU,
     same arrival trace.
 
@@ -644,7 +645,7 @@ def bench_serving(zk, torch, dev: int, njobs: int = 1000, rate: float = 2000.0, 
     def pct(x, q):
         return float(np.percentile(np.asarray(x), q)) if len(x) else None
 
-    srv = zk.Server(device=dev, hbm_budget=150 * 10**9, max_wave_jobs=wave_jobs)
+    srv = zk.Server(device=dev, hbm_budget=hbm_budget, max_wave_jobs=wave_jobs)
     bid = srv.add_bases(bases)
 
     def run_server(offered, jobs_idx=None, outs=None):
