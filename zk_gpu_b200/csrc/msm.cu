@@ -201,46 +201,139 @@ __device__ __forceinline__ void fq_inv_rp_bin(uint32_t r[8], const uint32_t a[8]
   reduce_once<FqP>(r, r);
 }
 
-// the point at position pos of a round's input: round 0 gathers the signed
-// base named by the sorted entry list, later rounds read their own buffer
+// ---- per-thread copy pipeline ---------------------------------------------
+// The prefix and apply passes are chains of dependent gathers (bucket
+// metadata -> entry list -> point) and field products.  Each thread stages
+// the operands of its next pair sum into shared memory with cp.async (16-B
+// copies that hold no registers while in flight) while it computes the
+// current one, and loads the entry-list words one job further ahead, so the
+// gather latency overlaps the products.  Stage slots are chunk-major: chunk
+// k of stage s of thread t is the 16-B word ((s * CH + k) * blockDim + t),
+// so the 16-B accesses of a warp to one chunk are 32 consecutive words.
+__device__ __forceinline__ void cp16(uint4* smem, const void* gmem) {
+  const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// one fe (two chunks) of a stage: copy in, read out
+__device__ __forceinline__ void cp_fe(uint4* my, uint32_t bd, uint32_t k, const fe* g) {
+  const uint4* v = reinterpret_cast<const uint4*>(g);
+  cp16(my + k * bd, v);
+  cp16(my + (k + 1) * bd, v + 1);
+}
+__device__ __forceinline__ void sm_fe(uint32_t r[8], const uint4* my, uint32_t bd, uint32_t k) {
+  const uint4 x = my[k * bd], y = my[(k + 1) * bd];
+  r[0] = x.x; r[1] = x.y; r[2] = x.z; r[3] = x.w;
+  r[4] = y.x; r[5] = y.y; r[6] = y.z; r[7] = y.w;
+}
+
+// one pair sum of a round: its two points in the round's source (round 0:
+// entry-list words, base index plus sign bit; later rounds: positions in the
+// previous round's output), its bucket, and whether the second point exists
+constexpr uint32_t BA_CP = 4;   // chunks per prefix stage: x of both points
+constexpr uint32_t BA_CA = 10;  // chunks per apply stage: both points, one prefix product
+struct BaJob {
+  uint32_t pa, pb, b;
+  bool has2;
+};
+
 template <bool FIRST>
-__device__ __forceinline__ void ba_load(aff_t& p, const fe* src, const uint32_t* list, uint32_t pos) {
+__device__ __forceinline__ BaJob ba_job(uint32_t q, uint32_t b, const uint32_t* __restrict__ joff,
+                                        const uint32_t* __restrict__ in_off, const uint32_t* __restrict__ cprev,
+                                        const uint32_t* __restrict__ list) {
+  BaJob d;
+  const uint32_t j = q - joff[b];
+  const uint32_t i0 = in_off[b] + 2 * j;
+  d.b = b;
+  d.has2 = 2 * j + 1 < cprev[b];
   if (FIRST) {
-    const uint32_t e = list[pos];
-    ld_aff(p, src + 2 * (uint64_t)(e & 0x7fffffffu));
-    if ((e & 0x80000000u) && !is_zero(p.x)) {
-      uint32_t z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-      sub<FqP>(p.y, z, p.y);
-    }
+    d.pa = list[i0];
+    d.pb = d.has2 ? list[i0 + 1] : 0u;
   } else {
-    ld_aff(p, src + 2 * (uint64_t)pos);
+    d.pa = i0;
+    d.pb = i0 + 1;
   }
+  return d;
 }
 template <bool FIRST>
-__device__ __forceinline__ void ba_load_x(uint32_t x[8], const fe* src, const uint32_t* list, uint32_t pos) {
-  if (FIRST)
-    ld_fe(x, src + 2 * (uint64_t)(list[pos] & 0x7fffffffu));
-  else
-    ld_fe(x, src + 2 * (uint64_t)pos);
+__device__ __forceinline__ const fe* ba_pt(const fe* src, uint32_t p) {
+  return src + 2 * (uint64_t)(FIRST ? (p & 0x7fffffffu) : p);
+}
+// y of a round-0 point read out of its slot: negated for a negative digit
+template <bool FIRST>
+__device__ __forceinline__ void ba_sign(aff_t& p, uint32_t e) {
+  if (FIRST && (e & 0x80000000u) && !is_zero(p.x)) {
+    uint32_t z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    sub<FqP>(p.y, z, p.y);
+  }
+}
+
+// bucket of job q: the largest b' with joff[b'] <= q, searched from the
+// bucket of a neighbouring job (forward: joff[b] <= q; backward: q < joff[b + 1])
+__device__ __forceinline__ uint32_t ba_search(const uint32_t* __restrict__ joff, uint32_t lo, uint32_t hi,
+                                              uint32_t q) {
+  while (hi - lo > 1) {  // joff[lo] <= q < joff[hi]
+    const uint32_t mid = (lo + hi) >> 1;
+    if (joff[mid] <= q) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+__device__ __forceinline__ uint32_t ba_bucket_fwd(const uint32_t* __restrict__ joff, uint32_t T, uint32_t b,
+                                                  uint32_t q) {
+  if (joff[b + 1] > q) return b;
+  if (b + 2 <= T && joff[b + 2] > q) return b + 1;
+  return ba_search(joff, b + 1, T, q);
+}
+__device__ __forceinline__ uint32_t ba_bucket_bwd(const uint32_t* __restrict__ joff, uint32_t b, uint32_t q) {
+  if (joff[b] <= q) return b;
+  if (joff[b - 1] <= q) return b - 1;
+  return ba_search(joff, 0, b - 1, q);
+}
+
+// stage the x coordinates of a job's points (prefix pass)
+template <bool FIRST>
+__device__ __forceinline__ void ba_stage_x(uint4* st, uint32_t bd, const fe* src, const BaJob& d) {
+  if (!d.has2) return;
+  cp_fe(st, bd, 0, ba_pt<FIRST>(src, d.pa));
+  cp_fe(st, bd, 2, ba_pt<FIRST>(src, d.pb));
+}
+// stage both points of a job and the prefix product before it (apply pass)
+template <bool FIRST>
+__device__ __forceinline__ void ba_stage_pq(uint4* st, uint32_t bd, const fe* src, const BaJob& d, const fe* p) {
+  const fe* a = ba_pt<FIRST>(src, d.pa);
+  cp_fe(st, bd, 0, a);
+  cp_fe(st, bd, 2, a + 1);
+  if (d.has2) {
+    const fe* c = ba_pt<FIRST>(src, d.pb);
+    cp_fe(st, bd, 4, c);
+    cp_fe(st, bd, 6, c + 1);
+  }
+  if (p) cp_fe(st, bd, 8, p);
 }
 
 // denominator of one pair sum (R' one when no inversion is needed: a carried
-// point, an identity operand, or P = -Q)
+// point, an identity operand, or P = -Q), from the staged x coordinates;
+// equal x (doubling or P = -Q, rare) reads both points again for y
 template <bool FIRST>
-__device__ __forceinline__ void ba_denominator(uint32_t d[8], const fe* src, const uint32_t* list, uint32_t i0,
-                                               bool has2) {
-  if (has2) {
+__device__ __forceinline__ void ba_denominator(uint32_t d[8], const uint4* st, uint32_t bd, const fe* src,
+                                               const BaJob& job) {
+  if (job.has2) {
     uint32_t x1[8], x2[8];
-    ba_load_x<FIRST>(x1, src, list, i0);
-    ba_load_x<FIRST>(x2, src, list, i0 + 1);
+    sm_fe(x1, st, bd, 0);
+    sm_fe(x2, st, bd, 2);
     if (!is_zero(x1) && !is_zero(x2)) {
       if (!eq(x1, x2)) {
         sub<FqP>(d, x2, x1);
         return;
       }
       aff_t p, q;
-      ba_load<FIRST>(p, src, list, i0);
-      ba_load<FIRST>(q, src, list, i0 + 1);
+      ld_aff(p, ba_pt<FIRST>(src, job.pa));
+      ld_aff(q, ba_pt<FIRST>(src, job.pb));
+      ba_sign<FIRST>(p, job.pa);
+      ba_sign<FIRST>(q, job.pb);
       if (eq(p.y, q.y)) {
         add<FqP>(d, p.y, p.y);
         return;
@@ -248,16 +341,6 @@ __device__ __forceinline__ void ba_denominator(uint32_t d[8], const fe* src, con
     }
   }
   fq_one_rp(d);
-}
-
-// largest bucket b < T with joff[b] <= q (joff: exclusive scan of jobs)
-__device__ __forceinline__ uint32_t ba_bucket_of(const uint32_t* joff, uint32_t T, uint32_t q) {
-  uint32_t lo = 0, hi = T;
-  while (hi - lo > 1) {
-    const uint32_t mid = (lo + hi) >> 1;
-    if (joff[mid] <= q) lo = mid; else hi = mid;
-  }
-  return lo;
 }
 
 // buckets with at most one entry are final before any round; every count
@@ -270,7 +353,9 @@ __global__ void ba_setup_kernel(const uint32_t* counts, const uint32_t* offsets,
   cnt[b] = c;
   if (c == 1) {
     aff_t p;
-    ba_load<true>(p, bases, list, offsets[b]);
+    const uint32_t e = list[offsets[b]];
+    ld_aff(p, ba_pt<true>(bases, e));
+    ba_sign<true>(p, e);
     st_fe(fin + 2 * (uint64_t)b, p.x);
     st_fe(fin + 2 * (uint64_t)b + 1, p.y);
   } else if (c == 0) {
@@ -296,31 +381,54 @@ __device__ __forceinline__ uint32_t ba_task_len(uint32_t J, uint32_t fill_k) {
   return max(1u, min(BA_K, J / fill_k));
 }
 
+// dynamic shared memory: 2 stages x BA_CP chunks x 16 B per thread
 template <bool FIRST>
-__global__ void __launch_bounds__(256) ba_prefix_kernel(const fe* src, const uint32_t* list, const uint32_t* in_off,
-                                                        const uint32_t* cprev, const uint32_t* joff,
-                                                        const uint32_t* np, uint32_t T, fe* pre, fe* tot,
+__global__ void __launch_bounds__(256) ba_prefix_kernel(const fe* __restrict__ src, const uint32_t* __restrict__ list,
+                                                        const uint32_t* __restrict__ in_off,
+                                                        const uint32_t* __restrict__ cprev,
+                                                        const uint32_t* __restrict__ joff, uint32_t T,
+                                                        fe* __restrict__ pre, fe* __restrict__ tot,
                                                         uint32_t fill_k) {
+  extern __shared__ uint4 ba_smem[];
+  const uint32_t bd = blockDim.x;
+  uint4* my = ba_smem + threadIdx.x;
   const uint32_t J = joff[T];
   const uint32_t K = ba_task_len(J, fill_k);
   const uint32_t tasks = (J + K - 1) / K;
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < tasks; t += gridDim.x * blockDim.x) {
     const uint32_t q0 = t * K, q1 = min(q0 + K, J);
-    uint32_t b = ba_bucket_of(joff, T, q0);
+    uint32_t b = ba_search(joff, 0, T, q0);
+    BaJob d0 = ba_job<FIRST>(q0, b, joff, in_off, cprev, list), d1 = d0;
+    ba_stage_x<FIRST>(my, bd, src, d0);
+    cp_commit();
+    if (q0 + 1 < q1) {
+      b = ba_bucket_fwd(joff, T, b, q0 + 1);
+      d1 = ba_job<FIRST>(q0 + 1, b, joff, in_off, cprev, list);
+    }
     uint32_t acc[8];
     for (uint32_t q = q0; q < q1; q++) {
-      if (q - joff[b] >= np[b]) b = ba_bucket_of(joff, T, q);
-      const uint32_t j = q - joff[b];
+      const uint32_t s = (q - q0) & 1;
+      if (q + 1 < q1) ba_stage_x<FIRST>(my + (s ^ 1) * BA_CP * bd, bd, src, d1);
+      cp_commit();
+      BaJob d2 = d1;
+      if (q + 2 < q1) {
+        b = ba_bucket_fwd(joff, T, b, q + 2);
+        d2 = ba_job<FIRST>(q + 2, b, joff, in_off, cprev, list);
+      }
+      cp_wait<1>();
       uint32_t d[8];
-      ba_denominator<FIRST>(d, src, list, in_off[b] + 2 * j, 2 * j + 1 < cprev[b]);
+      ba_denominator<FIRST>(d, my + s * BA_CP * bd, bd, src, d0);
       if (q == q0)
         cpy(acc, d);
       else
         qmul(acc, acc, d);
       st_fe(pre + q, acc);
+      d0 = d1;
+      d1 = d2;
     }
     st_fe(tot + t, acc);
   }
+  cp_wait<0>();
 }
 
 // invert: thread s turns tot[s G .. s G + G) into their inverses.  The
@@ -358,12 +466,21 @@ __global__ void __launch_bounds__(128) ba_invert_kernel(fe* tot, fe* tpre, const
   }
 }
 
-// apply: walk each task's chain back and finish its pair sums
+// apply: walk each task's chain back and finish its pair sums; dynamic
+// shared memory: 2 stages x BA_CA chunks x 16 B per thread
 template <bool FIRST>
-__global__ void __launch_bounds__(256) ba_apply_kernel(const fe* src, const uint32_t* list, const uint32_t* in_off,
-                                                       const uint32_t* cprev, const uint32_t* joff,
-                                                       const uint32_t* np, uint32_t T, const fe* pre, const fe* tot,
-                                                       fe* dst, fe* fin, uint32_t* cnt, uint32_t fill_k) {
+__global__ void __launch_bounds__(256, 2) ba_apply_kernel(const fe* __restrict__ src,
+                                                          const uint32_t* __restrict__ list,
+                                                          const uint32_t* __restrict__ in_off,
+                                                          const uint32_t* __restrict__ cprev,
+                                                          const uint32_t* __restrict__ joff,
+                                                          const uint32_t* __restrict__ np, uint32_t T,
+                                                          const fe* __restrict__ pre, const fe* __restrict__ tot,
+                                                          fe* __restrict__ dst, fe* __restrict__ fin,
+                                                          uint32_t* __restrict__ cnt, uint32_t fill_k) {
+  extern __shared__ uint4 ba_smem[];
+  const uint32_t bd = blockDim.x;
+  uint4* my = ba_smem + threadIdx.x;
   const uint32_t J = joff[T];
   const uint32_t K = ba_task_len(J, fill_k);
   const uint32_t tasks = (J + K - 1) / K;
@@ -371,15 +488,35 @@ __global__ void __launch_bounds__(256) ba_apply_kernel(const fe* src, const uint
     const uint32_t q0 = t * K, q1 = min(q0 + K, J);
     uint32_t inv_run[8];
     ld_fe(inv_run, tot + t);
-    uint32_t b = ba_bucket_of(joff, T, q1 - 1);
-    for (uint32_t q = q1; q-- > q0;) {
-      if (q < joff[b]) b = ba_bucket_of(joff, T, q);
-      const uint32_t j = q - joff[b], c = cprev[b];
-      const uint32_t i0 = in_off[b] + 2 * j;
-      const bool has2 = 2 * j + 1 < c;
+    uint32_t b = ba_search(joff, 0, T, q1 - 1);
+    BaJob d0 = ba_job<FIRST>(q1 - 1, b, joff, in_off, cprev, list), d1 = d0;
+    ba_stage_pq<FIRST>(my, bd, src, d0, q1 - 1 > q0 ? pre + q1 - 2 : nullptr);
+    cp_commit();
+    if (q1 - 1 > q0) {
+      b = ba_bucket_bwd(joff, b, q1 - 2);
+      d1 = ba_job<FIRST>(q1 - 2, b, joff, in_off, cprev, list);
+    }
+    for (uint32_t q = q1, i = 0; q-- > q0; i++) {
+      const uint32_t s = i & 1;
+      if (q > q0) ba_stage_pq<FIRST>(my + (s ^ 1) * BA_CA * bd, bd, src, d1, q - 1 > q0 ? pre + q - 2 : nullptr);
+      cp_commit();
+      BaJob d2 = d1;
+      if (q > q0 + 1) {
+        b = ba_bucket_bwd(joff, b, q - 2);
+        d2 = ba_job<FIRST>(q - 2, b, joff, in_off, cprev, list);
+      }
+      cp_wait<1>();
+      const uint4* st = my + s * BA_CA * bd;
+      const bool has2 = d0.has2;
       aff_t P, Q, out;
-      ba_load<FIRST>(P, src, list, i0);
-      if (has2) ba_load<FIRST>(Q, src, list, i0 + 1);
+      sm_fe(P.x, st, bd, 0);
+      sm_fe(P.y, st, bd, 2);
+      ba_sign<FIRST>(P, d0.pa);
+      if (has2) {
+        sm_fe(Q.x, st, bd, 4);
+        sm_fe(Q.y, st, bd, 6);
+        ba_sign<FIRST>(Q, d0.pb);
+      }
       // the same denominator the prefix pass chained (ba_denominator)
       uint32_t d[8];
       int kind = 0;  // 0: no inversion, 1: addition, 2: doubling
@@ -396,7 +533,7 @@ __global__ void __launch_bounds__(256) ba_apply_kernel(const fe* src, const uint
       uint32_t inv_d[8];
       if (q > q0) {
         uint32_t p[8];
-        ld_fe(p, pre + q - 1);
+        sm_fe(p, st, bd, 8);
         qmul(inv_d, inv_run, p);
         qmul(inv_run, inv_run, d);
       } else {
@@ -429,13 +566,16 @@ __global__ void __launch_bounds__(256) ba_apply_kernel(const fe* src, const uint
         qsub(out.y, t1, P.y);
         reduce_once<FqP>(out.y, out.y);
       }
-      const uint32_t nb = np[b];
-      fe* o = nb == 1 ? fin + 2 * (uint64_t)b : dst + 2 * (uint64_t)(joff[b] + j);
+      const uint32_t bq = d0.b, nb = np[bq];
+      fe* o = nb == 1 ? fin + 2 * (uint64_t)bq : dst + 2 * (uint64_t)q;
       st_fe(o, out.x);
       st_fe(o + 1, out.y);
-      if (j == 0) cnt[b] = nb;
+      if (q == joff[bq]) cnt[bq] = nb;
+      d0 = d1;
+      d1 = d2;
     }
   }
+  cp_wait<0>();
 }
 
 // Tail: what the rounds left (a few points per bucket, or many in a skewed
@@ -457,7 +597,7 @@ __global__ void __launch_bounds__(256) ba_fold_kernel(const uint32_t* cnt, const
                                                       uint32_t T, fe* chunk_res) {
   const uint32_t C = coff[T];
   for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < C; u += gridDim.x * blockDim.x) {
-    const uint32_t b = ba_bucket_of(coff, T, u);
+    const uint32_t b = ba_search(coff, 0, T, u);
     const uint32_t k = u - coff[b], c = cnt[b];
     xyzz_t acc;
     xyzz_set_inf(acc);
@@ -651,6 +791,22 @@ uint64_t ba_tasks_bound(uint64_t jb, uint64_t fill_k) {
 }
 constexpr uint32_t kFillK = 148 * 64;  // task threads that fill a B200 (148 SMs) at 64 per SM
 
+// dynamic shared memory of the round kernels at 256 threads (two stages)
+constexpr int kPrefixSmem = 2 * BA_CP * 16 * 256;  // 32 KiB
+constexpr int kApplySmem = 2 * BA_CA * 16 * 256;   // 80 KiB: above the 48 KiB default, opted in per device
+
+cudaError_t ba_kernel_attrs(int device) {
+  static std::mutex mu;
+  static uint64_t done = 0;  // one bit per device
+  std::lock_guard<std::mutex> lk(mu);
+  if (device < 64 && (done >> device) & 1) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(ba_apply_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kApplySmem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(ba_apply_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kApplySmem);
+  if (e == cudaSuccess && device < 64) done |= 1ull << device;
+  return e;
+}
+
 // Buffer sizes of one MSM pass (msm_run_impl allocates exactly these;
 // msm_scratch_bytes reports them for admission).
 struct MsmLayout {
@@ -782,6 +938,11 @@ cudaError_t msm_run_impl(const fe* d_scalars, const fe* d_bases, uint64_t n, fe*
     alloc((void**)&winsum, W * 128ull);
   if (!bases_rp_given) alloc((void**)&bases_rp, nbases * 64ull);
   if (e == cudaSuccess) {
+    int dev = 0;
+    e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = ba_kernel_attrs(dev);
+  }
+  if (e == cudaSuccess) {
     const double nd = (double)n;
     const int sms = sm_count();
     const uint32_t fill_k = kFillK;  // matches the task buffers' bound (layout)
@@ -832,16 +993,16 @@ cudaError_t msm_run_impl(const fe* d_scalars, const fe* d_bases, uint64_t n, fe*
         const uint64_t groups = tasks < fill ? tasks : std::max<uint64_t>(2ull * fill, tasks / BA_G + 1);
         const unsigned gi = (unsigned)std::min<uint64_t>((groups + 127) / 128, (uint64_t)sms * 8);
         if (first)
-          ba_prefix_kernel<true><<<gt, 256, 0, s>>>(src, list, in_off, cprev, jo, np, T, pre, tot, fill_k);
+          ba_prefix_kernel<true><<<gt, 256, kPrefixSmem, s>>>(src, list, in_off, cprev, jo, T, pre, tot, fill_k);
         else
-          ba_prefix_kernel<false><<<gt, 256, 0, s>>>(src, list, in_off, cprev, jo, np, T, pre, tot, fill_k);
+          ba_prefix_kernel<false><<<gt, 256, kPrefixSmem, s>>>(src, list, in_off, cprev, jo, T, pre, tot, fill_k);
         ba_invert_kernel<<<gi, 128, 0, s>>>(tot, tpre, jo, T, fill, fill_k);
         if (first)
-          ba_apply_kernel<true><<<gt, 256, 0, s>>>(src, list, in_off, cprev, jo, np, T, pre, tot, dst, fin, cnt,
-                                                   fill_k);
+          ba_apply_kernel<true><<<gt, 256, kApplySmem, s>>>(src, list, in_off, cprev, jo, np, T, pre, tot, dst, fin,
+                                                            cnt, fill_k);
         else
-          ba_apply_kernel<false><<<gt, 256, 0, s>>>(src, list, in_off, cprev, jo, np, T, pre, tot, dst, fin, cnt,
-                                                    fill_k);
+          ba_apply_kernel<false><<<gt, 256, kApplySmem, s>>>(src, list, in_off, cprev, jo, np, T, pre, tot, dst, fin,
+                                                             cnt, fill_k);
         nl += 7;
         jb = jb / 2 + T;
       }
