@@ -1,5 +1,5 @@
-// Host driver for tests/test_fq_inv.py: runs the library's branch-free binary
-// Fq inversion (zk_gpu_b200/csrc/fq_inv.cuh, the same code the MSM kernels
+// Host driver for tests/test_fq_inv.py: runs the library's branch-free
+// divstep Fq inversion (zk_gpu_b200/csrc/fq_inv.cuh, the same code the MSM kernels
 // run) on values read from stdin (hex, one per line) and prints the inverses.
 #include <cstdint>
 #include <cstdio>
@@ -13,7 +13,7 @@ int main() {
     uint32_t a[8] = {0}, r[8];
     // 64 hex digits, most significant first
     for (int i = 0; i < 8; i++) std::sscanf(line + 8 * (7 - i), "%8x", &a[i]);
-    zk::fq_inv_binary(r, a);
+    zk::fq_inv_divsteps(r, a);
     for (int i = 7; i >= 0; i--) std::printf("%08x", r[i]);
     std::printf("\n");
   }

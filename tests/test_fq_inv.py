@@ -1,6 +1,6 @@
-"""CPU: the MSM's branch-free binary Fq inversion (fq_inv.cuh, compiled for
+"""CPU: the MSM's branch-free divstep Fq inversion (fq_inv.cuh, compiled for
 the host from the same source the kernels use) against Python bigints, on
-random values and the edges 1, 2, (q-1)/2, q-1."""
+random values, the edges 1, 2, (q-1)/2, q-1, and long runs of equal bits."""
 import os
 import random
 import shutil
@@ -13,11 +13,13 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 
 @pytest.mark.skipif(shutil.which("g++") is None, reason="needs g++")
-def test_binary_inversion_matches_bigint(tmp_path):
+def test_divstep_inversion_matches_bigint(tmp_path):
     exe = tmp_path / "fq_inv_check"
     subprocess.run(["g++", "-O2", "-std=c++17", "-o", str(exe), os.path.join(HERE, "fq_inv_check.cpp")], check=True)
     rng = random.Random(2024)
     vals = [1, 2, 3, (Q - 1) // 2, Q - 2, Q - 1, 1 << 253, (1 << 254) % Q] + [rng.randrange(1, Q) for _ in range(3000)]
+    # powers of two, all-ones patterns and q - 2^k: long runs of equal bits
+    vals += [1 << k for k in range(254)] + [(1 << k) - 1 for k in range(2, 254)] + [Q - (1 << k) for k in range(253)]
     inp = "".join(f"{v:064x}\n" for v in vals)
     out = subprocess.run([str(exe)], input=inp, capture_output=True, text=True, check=True).stdout.split()
     assert len(out) == len(vals)

@@ -1,206 +1,196 @@
-// fq_inv.cuh — Fq inversion by the binary extended Euclidean algorithm in a
-// fixed number of branch-free steps, for the MSM's batch-affine rounds.
+// fq_inv.cuh — Fq inversion by Bernstein–Yang divsteps in a fixed number of
+// branch-free steps, for the MSM's batch-affine rounds.
 //
-// A Fermat inversion a^(q-2) is ~330 dependent Montgomery products: about
-// 0.18 ms of latency per inversion on the FP64 product, which sets a floor
-// under every batch-affine round.  Stein's binary algorithm needs only
-// additions, subtractions and shifts: with u = a, v = q, x1 = 1, x2 = 0 and
-// the invariants x1 a = u, x2 a = v (mod q), v odd, one step does
-//   if u is odd: (u, v, x1, x2) <- u < v ? (v - u, u, x2 - x1, x1)
-//                                        : (u - v, v, x1 - x2, x2)
-//   u <- u / 2,  x1 <- x1 / 2 mod q
-// Each step at least halves u v < q^2 < 2^508, so after 508 steps u = 0 and
-// v = gcd(a, q) = 1, x2 = a^-1.  Every step is the same instruction sequence
-// (masks, no branches), so the threads of a warp inverting different values
-// never diverge.  __host__ __device__: the host tests run the same code.
+// A Fermat inversion a^(q-2) is ~330 dependent Montgomery products (about
+// 0.18 ms of latency on the FP64 product); Stein's binary algorithm needs
+// ~500 steps of 256-bit subtractions, selects and shifts (~10^5
+// instructions).  The divstep recurrence of D. J. Bernstein and B.-Y. Yang,
+// "Fast constant-time gcd computation and modular inversion" (TCHES 2019),
+//   delta > 0 and g odd: (delta, f, g) <- (1 - delta, g, (g - f) / 2)
+//   g odd:               (delta, f, g) <- (1 + delta, f, (g + f) / 2)
+//   g even:              (delta, f, g) <- (1 + delta, f, g / 2)
+// starting from delta = 1, f = q (odd), g = a, reaches g = 0, f = +-1 after
+// at most floor((49 d + 57) / 17) = 741 steps for d = 256-bit inputs
+// (the paper's Theorem 11.2).  Each step looks only at the low bit of g,
+// so 30 steps run on the low 32 bits of f and g alone and yield a 2x2
+// integer matrix T with [f', g'] 2^30 = T [f, g]; the full-width numbers
+// are updated once per 30 steps.  The cofactors d, e with f = d a and
+// g = e a (mod q) follow the same matrix, divided by 2^30 modulo q
+// (adding the multiple of q that clears the low 30 bits).  At the end
+// a^-1 = f d (mod q).  25 batches (750 steps) and a bounded safety loop
+// on g != 0; every step is the same instruction sequence (masks, no
+// branches), so a warp's threads inverting different values never diverge.
+//
+// Numbers are signed radix-2^30 integers in 9 int32 limbs: limbs 0..7 in
+// [0, 2^30), limb 8 signed, 270 bits.  |f|, |g| <= q < 2^254 throughout;
+// |d|, |e| grow by less than q per batch (|u| + |v| <= 2^30 for the rows
+// of T), so they stay below 30 q < 2^259 and every limb product plus
+// carries fits an int64.  __host__ __device__: the host tests run the same
+// code as the kernels.
 #pragma once
 #include <cstdint>
 
 namespace zk {
+namespace fqinv {
 
-struct FqInvConst {
-  static constexpr uint32_t Q[8] = {0xd87cfd47u, 0x3c208c16u, 0x6871ca8du, 0x97816a91u,
-                                    0x8181585du, 0xb85045b6u, 0xe131a029u, 0x30644e72u};
-};
+constexpr int32_t M30 = (1 << 30) - 1;
+// limb i of q in radix 2^30 (a function: constant after unrolling, and
+// usable in device code, unlike a namespace-scope array), and -q^-1 mod 2^30
+__host__ __device__ constexpr int32_t QL(int i) {
+  return i == 0 ? 0x187cfd47 : i == 1 ? 0x3082305b : i == 2 ? 0x071ca8d3 : i == 3 ? 0x205aa45a
+       : i == 4 ? 0x01585d97 : i == 5 ? 0x0116da06 : i == 6 ? 0x1a029b85 : i == 7 ? 0x139cb84c : 0x3064;
+}
+constexpr uint32_t QNEG_INV30 = 0x24866389u;
+constexpr int kBatches = 25;  // 750 divsteps >= 741
 
-// r = a^-1 mod q for a canonical, nonzero a (plain integers, 8 x 32-bit
-// little-endian limbs); r is canonical.  a = 0 gives r = 0.
-__host__ __device__ inline void fq_inv_binary(uint32_t r[8], const uint32_t a[8]) {
-  constexpr uint32_t Q0 = 0xd87cfd47u, Q1 = 0x3c208c16u, Q2 = 0x6871ca8du, Q3 = 0x97816a91u, Q4 = 0x8181585du,
-                     Q5 = 0xb85045b6u, Q6 = 0xe131a029u, Q7 = 0x30644e72u;
-  const uint32_t q[8] = {Q0, Q1, Q2, Q3, Q4, Q5, Q6, Q7};
-  uint32_t u[8], v[8], x1[8], x2[8];
-  for (int i = 0; i < 8; i++) {
-    u[i] = a[i];
-    v[i] = q[i];
-    x1[i] = i == 0 ? 1u : 0u;
-    x2[i] = 0u;
+// 30 divsteps on the low 32 bits of f and g: returns the new delta and the
+// matrix T = [[u, v], [q, r]] with (f', g') 2^30 = (u f + v g, q f + r g)
+__host__ __device__ inline int32_t divsteps30(int32_t delta, uint32_t f, uint32_t g, int32_t t[4]) {
+  uint32_t u = 1, v = 0, q = 0, r = 1;
+#pragma unroll
+  for (int i = 0; i < 30; i++) {
+    const uint32_t godd = 0u - (g & 1u);
+    const uint32_t pos = (uint32_t)((int32_t)(0 - delta) >> 31);  // all ones iff delta > 0
+    const uint32_t sw = godd & pos;                               // the swapping case
+    // swap: (f, g) <- (g, g - f); g odd: (f, g + f); g even: (f, g); then g / 2
+    const uint32_t nf = (g & sw) | (f & ~sw), nu = (q & sw) | (u & ~sw), nv = (r & sw) | (v & ~sw);
+    g += ((f ^ sw) - sw) & godd;
+    q += ((u ^ sw) - sw) & godd;
+    r += ((v ^ sw) - sw) & godd;
+    f = nf;
+    u = nu << 1;
+    v = nv << 1;
+    g >>= 1;
+    delta = 1 + (int32_t)(((uint32_t)delta ^ sw) - sw);
   }
-  for (int step = 0; step < 508; step++) {
-    const uint32_t odd = u[0] & 1u;
-    // d = u - v; lt = u < v
-    uint32_t d[8];
-    uint64_t br = 0;
-    for (int i = 0; i < 8; i++) {
-      const uint64_t t = (uint64_t)u[i] - v[i] - br;
-      d[i] = (uint32_t)t;
-      br = (t >> 32) & 1u;
-    }
-    const uint32_t lt = (uint32_t)br;
-    const uint32_t m_odd = 0u - odd, m_swap = 0u - (odd & lt), m_lt = 0u - lt;
-    // |u - v|
-    uint32_t ad[8];
-    uint64_t c = lt;
-    for (int i = 0; i < 8; i++) {
-      const uint64_t t = (uint64_t)(d[i] ^ m_lt) + c;
-      ad[i] = (uint32_t)t;
-      c = t >> 32;
-    }
-    // x1 - x2 and x2 - x1 mod q
-    uint32_t dx[8], rx[8];
-    uint64_t b1 = 0, b2 = 0;
-    for (int i = 0; i < 8; i++) {
-      const uint64_t t1 = (uint64_t)x1[i] - x2[i] - b1;
-      const uint64_t t2 = (uint64_t)x2[i] - x1[i] - b2;
-      dx[i] = (uint32_t)t1;
-      rx[i] = (uint32_t)t2;
-      b1 = (t1 >> 32) & 1u;
-      b2 = (t2 >> 32) & 1u;
-    }
-    const uint32_t mb1 = 0u - (uint32_t)b1, mb2 = 0u - (uint32_t)b2;
-    uint64_t c1 = 0, c2 = 0;
-    for (int i = 0; i < 8; i++) {
-      const uint64_t t1 = (uint64_t)dx[i] + (q[i] & mb1) + c1;
-      const uint64_t t2 = (uint64_t)rx[i] + (q[i] & mb2) + c2;
-      dx[i] = (uint32_t)t1;
-      rx[i] = (uint32_t)t2;
-      c1 = t1 >> 32;
-      c2 = t2 >> 32;
-    }
-    // new v, x2 (swap case) and the new u, x1 before halving
-    uint32_t nu[8], nx[8];
-    for (int i = 0; i < 8; i++) {
-      const uint32_t vi = (u[i] & m_swap) | (v[i] & ~m_swap);
-      const uint32_t x2i = (x1[i] & m_swap) | (x2[i] & ~m_swap);
-      const uint32_t dxi = (rx[i] & m_lt) | (dx[i] & ~m_lt);
-      nu[i] = (ad[i] & m_odd) | (u[i] & ~m_odd);
-      nx[i] = (dxi & m_odd) | (x1[i] & ~m_odd);
-      v[i] = vi;
-      x2[i] = x2i;
-    }
-    // u <- u / 2 (u is even here); x1 <- x1 / 2 mod q
-    const uint32_t m_xodd = 0u - (nx[0] & 1u);
-    uint32_t hx[8];
-    uint64_t cx = 0;
-    for (int i = 0; i < 8; i++) {
-      const uint64_t t = (uint64_t)nx[i] + (q[i] & m_xodd) + cx;  // x + q < 2^255: no carry out
-      hx[i] = (uint32_t)t;
-      cx = t >> 32;
-    }
-    for (int i = 0; i < 7; i++) {
-      u[i] = (nu[i] >> 1) | (nu[i + 1] << 31);
-      x1[i] = (hx[i] >> 1) | (hx[i + 1] << 31);
-    }
-    u[7] = nu[7] >> 1;
-    x1[7] = hx[7] >> 1;
-  }
-  for (int i = 0; i < 8; i++) r[i] = x2[i];
+  t[0] = (int32_t)u;
+  t[1] = (int32_t)v;
+  t[2] = (int32_t)q;
+  t[3] = (int32_t)r;
+  return delta;
 }
 
-}  // namespace zk
-
-#ifdef __CUDACC__
-namespace zk {
-
-// The same algorithm for device code with every multi-word add / subtract a
-// single carry chain (sub.cc / subc, add.cc / addc) inside one asm statement:
-// a step's dependent path is a few short chains instead of emulated 64-bit
-// borrows, which cuts the inversion's latency several times.  Tested through
-// the MSM tests (every result bit-exact) and against fq_inv_binary's host
-// check by construction (identical step semantics).
-#define ZK_INV_SUB8(d, a, b, br)                                                                        \
-  asm("sub.cc.u32  %0, %9, %17;\n\tsubc.cc.u32 %1, %10, %18;\n\tsubc.cc.u32 %2, %11, %19;\n\t"          \
-      "subc.cc.u32 %3, %12, %20;\n\tsubc.cc.u32 %4, %13, %21;\n\tsubc.cc.u32 %5, %14, %22;\n\t"         \
-      "subc.cc.u32 %6, %15, %23;\n\tsubc.cc.u32 %7, %16, %24;\n\tsubc.u32 %8, 0, 0;"                     \
-      : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]), \
-        "=r"(br)                                                                                         \
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]),          \
-        "r"(b[0]), "r"(b[1]), "r"(b[2]), "r"(b[3]), "r"(b[4]), "r"(b[5]), "r"(b[6]), "r"(b[7]))
-// d += b (8 words, carry out dropped)
-#define ZK_INV_ADD8(d, b)                                                                               \
-  asm("add.cc.u32  %0, %0, %8;\n\taddc.cc.u32 %1, %1, %9;\n\taddc.cc.u32 %2, %2, %10;\n\t"              \
-      "addc.cc.u32 %3, %3, %11;\n\taddc.cc.u32 %4, %4, %12;\n\taddc.cc.u32 %5, %5, %13;\n\t"            \
-      "addc.cc.u32 %6, %6, %14;\n\taddc.u32 %7, %7, %15;"                                               \
-      : "+r"(d[0]), "+r"(d[1]), "+r"(d[2]), "+r"(d[3]), "+r"(d[4]), "+r"(d[5]), "+r"(d[6]), "+r"(d[7])  \
-      : "r"(b[0]), "r"(b[1]), "r"(b[2]), "r"(b[3]), "r"(b[4]), "r"(b[5]), "r"(b[6]), "r"(b[7]))
-
-__device__ __forceinline__ void fq_inv_binary_dev(uint32_t r[8], const uint32_t a[8]) {
-  const uint32_t q[8] = {0xd87cfd47u, 0x3c208c16u, 0x6871ca8du, 0x97816a91u,
-                         0x8181585du, 0xb85045b6u, 0xe131a029u, 0x30644e72u};
-  uint32_t u[8], v[8], x1[8], x2[8];
+// (f, g) <- (u f + v g, q f + r g) / 2^30, exact
+__host__ __device__ inline void update_fg(int32_t f[9], int32_t g[9], const int32_t t[4]) {
+  const int64_t u = t[0], v = t[1], q = t[2], r = t[3];
+  int64_t cf = u * f[0] + v * g[0], cg = q * f[0] + r * g[0];
+  cf >>= 30;
+  cg >>= 30;
 #pragma unroll
-  for (int i = 0; i < 8; i++) {
-    u[i] = a[i];
-    v[i] = q[i];
-    x1[i] = i == 0 ? 1u : 0u;
-    x2[i] = 0u;
+  for (int i = 1; i < 9; i++) {
+    cf += u * f[i] + v * g[i];
+    cg += q * f[i] + r * g[i];
+    f[i - 1] = (int32_t)(cf & M30);
+    g[i - 1] = (int32_t)(cg & M30);
+    cf >>= 30;
+    cg >>= 30;
   }
+  f[8] = (int32_t)cf;
+  g[8] = (int32_t)cg;
+}
+
+// (d, e) <- (u d + v e, q d + r e) / 2^30 mod q: each row plus m q, with m
+// in [0, 2^30) chosen to clear its low 30 bits, is then divided exactly
+__host__ __device__ inline void update_de(int32_t d[9], int32_t e[9], const int32_t t[4]) {
+  const int64_t u = t[0], v = t[1], q = t[2], r = t[3];
+  const uint32_t sd = (uint32_t)t[0] * (uint32_t)d[0] + (uint32_t)t[1] * (uint32_t)e[0];
+  const uint32_t se = (uint32_t)t[2] * (uint32_t)d[0] + (uint32_t)t[3] * (uint32_t)e[0];
+  const int64_t md = (int64_t)((sd * QNEG_INV30) & (uint32_t)M30);
+  const int64_t me = (int64_t)((se * QNEG_INV30) & (uint32_t)M30);
+  int64_t cd = u * d[0] + v * e[0] + md * QL(0), ce = q * d[0] + r * e[0] + me * QL(0);
+  cd >>= 30;
+  ce >>= 30;
+#pragma unroll
+  for (int i = 1; i < 9; i++) {
+    cd += u * d[i] + v * e[i] + md * QL(i);
+    ce += q * d[i] + r * e[i] + me * QL(i);
+    d[i - 1] = (int32_t)(cd & M30);
+    e[i - 1] = (int32_t)(ce & M30);
+    cd >>= 30;
+    ce >>= 30;
+  }
+  d[8] = (int32_t)cd;
+  e[8] = (int32_t)ce;
+}
+
+__host__ __device__ inline bool limbs_zero(const int32_t g[9]) {
+  int32_t o = 0;
+#pragma unroll
+  for (int i = 0; i < 9; i++) o |= g[i];
+  return o == 0;
+}
+
+}  // namespace fqinv
+
+// r = a^-1 mod q for a canonical a (plain integers, 8 x 32-bit little-endian
+// words); r is canonical.  a = 0 gives r = 0.
+__host__ __device__ inline void fq_inv_divsteps(uint32_t r[8], const uint32_t a[8]) {
+  using namespace fqinv;
+  int32_t f[9], g[9], d[9], e[9];
+#pragma unroll
+  for (int i = 0; i < 9; i++) {
+    f[i] = QL(i);
+    d[i] = 0;
+    e[i] = i == 0 ? 1 : 0;
+    // bits [30 i, 30 i + 30) of a
+    const int w = (30 * i) >> 5, b = (30 * i) & 31;
+    uint64_t x = a[w];
+    if (w + 1 < 8) x |= (uint64_t)a[w + 1] << 32;
+    g[i] = (int32_t)((x >> b) & (uint64_t)M30);
+  }
+  int32_t delta = 1;
 #pragma unroll 1
-  for (int step = 0; step < 508; step++) {
-    const uint32_t m_odd = 0u - (u[0] & 1u);
-    uint32_t d[8], m_lt;
-    ZK_INV_SUB8(d, u, v, m_lt);  // m_lt: all ones iff u < v
-    const uint32_t m_swap = m_odd & m_lt;
-    // |u - v| = (d ^ m) - m
-    uint32_t ad[8], neg1[8];
+  for (int it = 0; it < kBatches + 4; it++) {
+    if (it >= kBatches && limbs_zero(g)) break;  // the bound says g = 0 after kBatches
+    int32_t t[4];
+    delta = divsteps30(delta, (uint32_t)f[0] | ((uint32_t)f[1] << 30), (uint32_t)g[0] | ((uint32_t)g[1] << 30), t);
+    update_de(d, e, t);
+    update_fg(f, g, t);
+  }
+  // f = +-1 (limb 8 holds the sign): x = f d, then x + 32 q in (0, 64 q)
+  const int64_t s = f[8] < 0 ? -1 : 1;
+  int64_t c = 0;
+  int32_t x[9];
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
-      ad[i] = d[i] ^ m_lt;
-      neg1[i] = i == 0 ? (m_lt & 1u) : 0u;
+  for (int i = 0; i < 9; i++) {
+    c += s * d[i] + 32 * (int64_t)QL(i);
+    x[i] = (int32_t)(c & M30);
+    c >>= 30;
+  }
+  // radix 2^30 -> 9 words of 32 bits (the value is below 2^260)
+  uint32_t w[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    const int i = (32 * k) / 30, b = (32 * k) % 30;
+    uint64_t v = (uint64_t)(uint32_t)x[i] >> b;
+    if (i + 1 < 9) v |= (uint64_t)(uint32_t)x[i + 1] << (30 - b);
+    if (i + 2 < 9) v |= (uint64_t)(uint32_t)x[i + 2] << (60 - b);
+    w[k] = (uint32_t)v;
+  }
+  // subtract 32 q, 16 q, ..., q where it does not go negative: [0, q)
+  constexpr uint32_t Q[8] = {0xd87cfd47u, 0x3c208c16u, 0x6871ca8du, 0x97816a91u,
+                             0x8181585du, 0xb85045b6u, 0xe131a029u, 0x30644e72u};
+#pragma unroll
+  for (int k = 5; k >= 0; k--) {
+    uint32_t sh[9];
+    sh[0] = Q[0] << k;
+#pragma unroll
+    for (int i = 1; i < 8; i++) sh[i] = k ? (Q[i] << k) | (Q[i - 1] >> (32 - k)) : Q[i];
+    sh[8] = k ? Q[7] >> (32 - k) : 0u;
+    uint32_t t[9];
+    uint64_t br = 0;
+#pragma unroll
+    for (int i = 0; i < 9; i++) {
+      const uint64_t y = (uint64_t)w[i] - sh[i] - br;
+      t[i] = (uint32_t)y;
+      br = (y >> 63) & 1u;
     }
-    ZK_INV_ADD8(ad, neg1);
-    // x1 - x2 and x2 - x1, mod q
-    uint32_t dx[8], rx[8], b1, b2;
-    ZK_INV_SUB8(dx, x1, x2, b1);
-    ZK_INV_SUB8(rx, x2, x1, b2);
-    uint32_t q1[8], q2[8];
+    const uint32_t keep = 0u - (uint32_t)br;  // all ones: w < k q, keep w
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
-      q1[i] = q[i] & b1;
-      q2[i] = q[i] & b2;
-    }
-    ZK_INV_ADD8(dx, q1);
-    ZK_INV_ADD8(rx, q2);
-    uint32_t nu[8], nx[8];
-#pragma unroll
-    for (int i = 0; i < 8; i++) {
-      const uint32_t vi = (u[i] & m_swap) | (v[i] & ~m_swap);
-      const uint32_t x2i = (x1[i] & m_swap) | (x2[i] & ~m_swap);
-      const uint32_t dxi = (rx[i] & m_lt) | (dx[i] & ~m_lt);
-      nu[i] = (ad[i] & m_odd) | (u[i] & ~m_odd);
-      nx[i] = (dxi & m_odd) | (x1[i] & ~m_odd);
-      v[i] = vi;
-      x2[i] = x2i;
-    }
-    // u /= 2; x1 = x1 / 2 mod q
-    const uint32_t m_xodd = 0u - (nx[0] & 1u);
-    uint32_t qx[8];
-#pragma unroll
-    for (int i = 0; i < 8; i++) qx[i] = q[i] & m_xodd;
-    ZK_INV_ADD8(nx, qx);  // x + q < 2^255: no carry out
-#pragma unroll
-    for (int i = 0; i < 7; i++) {
-      u[i] = __funnelshift_r(nu[i], nu[i + 1], 1);
-      x1[i] = __funnelshift_r(nx[i], nx[i + 1], 1);
-    }
-    u[7] = nu[7] >> 1;
-    x1[7] = nx[7] >> 1;
+    for (int i = 0; i < 9; i++) w[i] = (w[i] & keep) | (t[i] & ~keep);
   }
 #pragma unroll
-  for (int i = 0; i < 8; i++) r[i] = x2[i];
+  for (int i = 0; i < 8; i++) r[i] = w[i];
 }
-#undef ZK_INV_SUB8
-#undef ZK_INV_ADD8
 
 }  // namespace zk
-#endif

@@ -174,9 +174,9 @@ __global__ void scan_add_kernel(uint32_t* out, uint32_t* cursor, const uint32_t*
 //             3 products).
 // That is about 6 + 3 / BA_K ~ 6.2 Fq products per point addition (the XYZZ
 // mixed addition costs 10) plus one inversion per 512 additions, done by
-// the branch-free binary algorithm of fq_inv.cuh (shifts and subtractions,
-// ~0.01 ms of latency against ~0.18 ms for a Fermat power), with no serial
-// block-wide step.  Equal x
+// the branch-free divstep algorithm of fq_inv.cuh (~25k instructions of
+// 32-bit integer work against ~330 dependent products for a Fermat power),
+// with no serial block-wide step.  Equal x
 // (P = Q: doubling, denominator 2y; P = -Q: identity) and the identity
 // (x = 0: no BN254 point has x = 0, as 3 is not a square mod q) are handled
 // per sum.  A bucket reaching one point writes it to `fin`; after the last
@@ -188,7 +188,7 @@ constexpr uint32_t BA_G = 32;  // task products per inversion
 
 __device__ __forceinline__ void fq_one_rp(uint32_t r[8]) { set_one_rp<FqP>(r); }
 
-// a^-1 for a != 0 in R' form (x 2^260), lazy in, canonical out: the binary
+// a^-1 for a != 0 in R' form (x 2^260), lazy in, canonical out: the divstep
 // inversion (fq_inv.cuh) of the representative a 2^260 gives a^-1 2^-260,
 // and one product with 2^780 mod q returns it to R' form.
 __device__ __forceinline__ void fq_inv_rp_bin(uint32_t r[8], const uint32_t a[8]) {
@@ -196,7 +196,7 @@ __device__ __forceinline__ void fq_inv_rp_bin(uint32_t r[8], const uint32_t a[8]
                             0x3603f972u, 0xc5387239u, 0x8d1987f5u, 0x10f16dedu};
   uint32_t c[8], t[8];
   reduce_once<FqP>(c, a);
-  fq_inv_binary_dev(t, c);
+  fq_inv_divsteps(t, c);
   qmul(r, t, k780);
   reduce_once<FqP>(r, r);
 }

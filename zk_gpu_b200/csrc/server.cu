@@ -234,7 +234,9 @@ class Server {
         // the device's table caches count against the budget too
         adm_.set_external(table_cache_bytes(device_));
         for (uint64_t t : adm_.admit(max_wave_)) batch.push_back(jobs_.at(t).get());
-        peak_ = std::max(peak_, adm_.used() + adm_.reserved() + adm_.external());
+        // the peak is what admitted work holds (tables other work cached
+        // before anything was admitted are dropped below, not counted)
+        if (!batch.empty()) peak_ = std::max(peak_, adm_.used() + adm_.reserved() + adm_.external());
         if (batch.empty()) {
           if (waves_inflight_ == 0 && adm_.external() > 0) {
             // nothing will retire to make room: drop the cached tables (work
