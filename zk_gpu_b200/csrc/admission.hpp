@@ -33,6 +33,12 @@ class AdmissionQueue {
     reserved_ += bytes;
     return true;
   }
+  // give back a reservation (resident bases that failed to load)
+  void unreserve(uint64_t bytes) {
+    bytes = bytes > reserved_ ? reserved_ : bytes;
+    reserved_ -= bytes;
+    budget_ += bytes;
+  }
   uint64_t reserved() const { return reserved_; }
   // device memory held outside the jobs (the library's table caches), set
   // before each admission round; it counts against the same budget

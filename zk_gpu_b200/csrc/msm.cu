@@ -28,12 +28,11 @@ MsmPlan make_msm_plan(uint64_t n, int c_override, int device) {
   p.c = c;
   p.windows = (254 + c - 1) / c;
   p.buckets = 1u << (c - 1);
-  // buckets per reduction segment: each segment thread's latency is its
-  // running sum (2L additions) plus the weight multiply lo * S (about c
-  // doublings).  Few buckets per window: short segments (L = 4) for
-  // parallelism; many (2^12 and up): L = 16, since the extra weight
-  // multiplies of 4x more segments cost more than they save (measured on
-  // B200: 2^14 points, c = 10: 0.57 -> 0.24 ms; 2^22, c = 15: 0.9 -> 1.6 ms)
+  // buckets per reduction segment: a segment thread's latency is its
+  // running sum (2L additions); the window kernel then walks B / L segment
+  // sums per window, M = B / (256 L) per thread.  Few buckets per window:
+  // L = 4 for parallelism; many (2^12 and up): L = 16, which keeps the
+  // per-window pass (one block per window) short
   p.seg_len = std::min<uint32_t>(p.buckets >= 4096 ? 16u : 4u, p.buckets);
   return p;
 }
@@ -210,9 +209,13 @@ __device__ __forceinline__ void fq_inv_rp_bin(uint32_t r[8], const uint32_t a[8]
 // gather latency overlaps the products.  Stage slots are chunk-major: chunk
 // k of stage s of thread t is the 16-B word ((s * CH + k) * blockDim + t),
 // so the 16-B accesses of a warp to one chunk are 32 consecutive words.
+// .cg: through L2 only; staged data is read once, so allocating it in L1
+// only evicts other lines.  (Round 0's random 32-B and 64-B gathers move
+// whole 128-B lines from DRAM either way: 6.5 GB of DRAM reads for 2.2 GB
+// of x coordinates in the 2^22-point prefix pass, measured on B200.)
 __device__ __forceinline__ void cp16(uint4* smem, const void* gmem) {
   const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
@@ -258,6 +261,12 @@ __device__ __forceinline__ BaJob ba_job(uint32_t q, uint32_t b, const uint32_t* 
   }
   return d;
 }
+// point p of a round's source ((x, y) adjacent): round 0 reads the bases
+// (the entry's index, sign bit cleared), later rounds their own buffer of
+// affine pair sums.  (Bases kept as an x array and a y array instead were
+// measured on B200 at 2^22 points: the prefix pass's x gathers hit L2 more,
+// 1.28 -> 1.15 ms, and the apply pass's separate y gathers cost as much,
+// 3.94 -> 4.06 ms.)
 template <bool FIRST>
 __device__ __forceinline__ const fe* ba_pt(const fe* src, uint32_t p) {
   return src + 2 * (uint64_t)(FIRST ? (p & 0x7fffffffu) : p);
@@ -665,11 +674,12 @@ __global__ void __launch_bounds__(256) ba_heavy_kernel(const uint32_t* coff, con
   }
 }
 
-// Per (window, segment): running sums over the segment's buckets, top down,
-// giving sum_j (j - lo + 1) B_j and sum_j B_j; result T + lo * S, which is
-// the segment's share of sum_j (j + 1) B_j.
-__global__ void __launch_bounds__(128) msm_segment_kernel(const fe* buckets, fe* segres, uint32_t B, uint32_t L,
-                                                          uint32_t total_segs) {
+// Bucket reduction.  A window's sum is W = sum_j (j + 1) B_j over its B
+// buckets.  Level 1, one thread per segment of L buckets: running sums from
+// the top give T_s = sum_i (i + 1) B_{sL+i} and S_s = sum_i B_{sL+i}, so
+// W = sum_s T_s + L sum_s s S_s.
+__global__ void __launch_bounds__(128) msm_segment_kernel(const fe* buckets, fe* seg_t, fe* seg_s, uint32_t B,
+                                                          uint32_t L, uint32_t total_segs) {
   const uint32_t gs = blockIdx.x * blockDim.x + threadIdx.x;
   if (gs >= total_segs) return;
   const uint32_t S_per_w = B / L;
@@ -683,35 +693,91 @@ __global__ void __launch_bounds__(128) msm_segment_kernel(const fe* buckets, fe*
     xyzz_add(run, bk);
     xyzz_add(tot, run);
   }
-  xyzz_mul_small(run, lo);
-  xyzz_add(tot, run);
-  st_xyzz(segres + 4 * (uint64_t)gs, tot);
+  st_xyzz(seg_t + 4 * (uint64_t)gs, tot);
+  st_xyzz(seg_s + 4 * (uint64_t)gs, run);
 }
 
-// One block per window: tree sum of its segment results.
-__global__ void __launch_bounds__(256) msm_window_kernel(const fe* segres, fe* winsum, uint32_t S_per_w) {
-  __shared__ fe sh[256 * 4];
-  const uint32_t w = blockIdx.x;
-  xyzz_t acc, t;
-  xyzz_set_inf(acc);
-  for (uint32_t s = threadIdx.x; s < S_per_w; s += blockDim.x) {
-    ld_xyzz(t, segres + 4 * ((uint64_t)w * S_per_w + s));
-    xyzz_add(acc, t);
+// Level 2, one block per window, thread t owning M consecutive segments
+// (S_per_w and the block size are powers of two): A_t = sum_k T_{tM+k},
+// U_t = sum_k k S_{tM+k} and V_t = sum_k S_{tM+k} by running sums, so that
+// sum_s s S_s = sum_t U_t + M sum_t t V_t, and sum_t t V_t = sum_{t>=1} P_t
+// with P_t = sum_{u>=t} V_u (a block suffix scan).  Thread t contributes
+// c_t = A_t + L U_t + L M P_t (no P term for t = 0); a tree sum gives W.
+// The serial depth is about M + 2 log2(256) additions and log2(L M)
+// doublings per window, against L + c doublings and additions per segment
+// for multiplying every segment sum by its offset (measured on B200, 2^22
+// points, c = 16: 1.16 ms for both levels against 1.25 ms).  The
+// accumulator not being added to waits in the thread's slot of shared
+// memory (two slot arrays, 64 KiB of dynamic shared memory), so at most
+// two points are live in registers.
+constexpr int kWindowSmem = 2 * 256 * 128;
+__global__ void __launch_bounds__(256) msm_window_kernel(const fe* seg_t, const fe* seg_s, fe* winsum,
+                                                         uint32_t S_per_w, uint32_t L) {
+  extern __shared__ uint4 win_smem[];
+  fe* sc = reinterpret_cast<fe*>(win_smem);  // per thread: c_t, then the tree
+  fe* sv = sc + 4 * blockDim.x;               // per thread: V_t, then the scan
+  const uint32_t w = blockIdx.x, t = threadIdx.x, nt = blockDim.x;
+  const uint32_t M = S_per_w > nt ? S_per_w / nt : 1u;
+  const uint32_t active = S_per_w / M;
+  xyzz_t a, x;
+  xyzz_set_inf(a);
+  st_xyzz(sc + 4 * t, a);  // U_t accumulates here
+  if (t < active) {
+    const uint64_t base = (uint64_t)w * S_per_w + (uint64_t)t * M;
+    // a = V (running), U in sc
+    for (uint32_t k = M - 1; k >= 1; k--) {
+      ld_xyzz(x, seg_s + 4 * (base + k));
+      xyzz_add(a, x);
+      ld_xyzz(x, sc + 4 * t);
+      xyzz_add(x, a);
+      st_xyzz(sc + 4 * t, x);
+    }
+    ld_xyzz(x, seg_s + 4 * base);
+    xyzz_add(a, x);
+    st_xyzz(sv + 4 * t, a);  // V_t
+    // a = L U_t + A_t
+    ld_xyzz(a, sc + 4 * t);
+    for (uint32_t m = L; m > 1; m >>= 1) xyzz_dbl(a, a);  // L a power of two
+    for (uint32_t k = 0; k < M; k++) {
+      ld_xyzz(x, seg_t + 4 * (base + k));
+      xyzz_add(a, x);
+    }
+  } else {
+    st_xyzz(sv + 4 * t, a);
   }
-  st_xyzz(sh + 4 * threadIdx.x, acc);
+  st_xyzz(sc + 4 * t, a);
   __syncthreads();
-  for (uint32_t half = blockDim.x / 2; half > 0; half >>= 1) {
-    if (threadIdx.x < half) {
-      ld_xyzz(acc, sh + 4 * threadIdx.x);
-      ld_xyzz(t, sh + 4 * (threadIdx.x + half));
-      xyzz_add(acc, t);
-      st_xyzz(sh + 4 * threadIdx.x, acc);
+  // suffix sums of V across the block
+  ld_xyzz(a, sv + 4 * t);
+  for (uint32_t off = 1; off < nt; off <<= 1) {
+    const bool has = t + off < nt;
+    if (has) ld_xyzz(x, sv + 4 * (t + off));
+    __syncthreads();
+    if (has) {
+      xyzz_add(a, x);
+      st_xyzz(sv + 4 * t, a);
     }
     __syncthreads();
   }
-  if (threadIdx.x == 0) {
-    ld_xyzz(acc, sh);
-    st_xyzz(winsum + 4 * (uint64_t)w, acc);
+  if (t > 0) {
+    for (uint32_t m = L * M; m > 1; m >>= 1) xyzz_dbl(a, a);  // L M P_t
+    ld_xyzz(x, sc + 4 * t);
+    xyzz_add(x, a);
+    st_xyzz(sc + 4 * t, x);
+  }
+  __syncthreads();
+  for (uint32_t half = nt / 2; half > 0; half >>= 1) {
+    if (t < half) {
+      ld_xyzz(a, sc + 4 * t);
+      ld_xyzz(x, sc + 4 * (t + half));
+      xyzz_add(a, x);
+      st_xyzz(sc + 4 * t, a);
+    }
+    __syncthreads();
+  }
+  if (t == 0) {
+    ld_xyzz(a, sc);
+    st_xyzz(winsum + 4 * (uint64_t)w, a);
   }
 }
 
@@ -794,6 +860,7 @@ constexpr uint32_t kFillK = 148 * 64;  // task threads that fill a B200 (148 SMs
 // dynamic shared memory of the round kernels at 256 threads (two stages)
 constexpr int kPrefixSmem = 2 * BA_CP * 16 * 256;  // 32 KiB
 constexpr int kApplySmem = 2 * BA_CA * 16 * 256;   // 80 KiB: above the 48 KiB default, opted in per device
+// (as is the window kernel's kWindowSmem, 64 KiB)
 
 cudaError_t ba_kernel_attrs(int device) {
   static std::mutex mu;
@@ -803,6 +870,8 @@ cudaError_t ba_kernel_attrs(int device) {
   cudaError_t e = cudaFuncSetAttribute(ba_apply_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kApplySmem);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(ba_apply_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kApplySmem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(msm_window_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kWindowSmem);
   if (e == cudaSuccess && device < 64) done |= 1ull << device;
   return e;
 }
@@ -825,7 +894,7 @@ struct MsmLayout {
     b += jb[0] * 64 + (rounds > 1 ? jb[1] * 64 : 0) + jb[0] * 32;  // round buffers, prefixes
     b += tasks0 * 32 * 2;                                         // task products, their prefixes
     b += T * 4ull * 2 + chunks * 128 + 4;                         // tail: chunk counts, heavy list, chunk sums
-    b += T * 128ull + segs * 128ull + (own_winsum ? W * 128ull : 0);
+    b += T * 128ull + segs * 256ull + (own_winsum ? W * 128ull : 0);  // buckets, segment T_s and S_s
     b += nbases_convert * 64;
     return b + 24 * 256;  // pool granularity per allocation
   }
@@ -904,7 +973,8 @@ cudaError_t msm_run_impl(const fe* d_scalars, const fe* d_bases, uint64_t n, fe*
   uint32_t *counts = nullptr, *offsets = nullptr, *cursor = nullptr, *bsums = nullptr, *list = nullptr;
   uint32_t *cnt = nullptr, *cprev = nullptr, *np = nullptr, *joff[2] = {nullptr, nullptr};
   fe *fin = nullptr, *buf[2] = {nullptr, nullptr}, *pre = nullptr, *tot = nullptr, *tpre = nullptr;
-  fe *buckets = nullptr, *segres = nullptr, *winsum = nullptr, *bases_rp = nullptr, *chunk_res = nullptr;
+  fe *buckets = nullptr, *segres = nullptr, *segsum = nullptr, *winsum = nullptr, *bases_rp = nullptr;
+  fe* chunk_res = nullptr;
   uint32_t *nch = nullptr, *heavy = nullptr, *heavy_count = nullptr;
   cudaError_t e = cudaSuccess;
   auto alloc = [&](void** ptr, size_t bytes) {
@@ -932,6 +1002,7 @@ cudaError_t msm_run_impl(const fe* d_scalars, const fe* d_bases, uint64_t n, fe*
   alloc((void**)&chunk_res, l.chunks * 128);
   alloc((void**)&buckets, T * 128ull);
   alloc((void**)&segres, segs * 128ull);
+  alloc((void**)&segsum, segs * 128ull);
   if (wout)
     winsum = wout->d_winsum;  // caller's buffer, left for the host's Horner step
   else
@@ -1023,16 +1094,16 @@ cudaError_t msm_run_impl(const fe* d_scalars, const fe* d_bases, uint64_t n, fe*
     }
     {
       ProfScope ps("msm_segment", s, (double)T * 2 * 14, T * 128.0);
-      msm_segment_kernel<<<(segs + 127) / 128, 128, 0, s>>>(buckets, segres, B, L, segs);
+      msm_segment_kernel<<<(segs + 127) / 128, 128, 0, s>>>(buckets, segres, segsum, B, L, segs);
     }
-    msm_window_kernel<<<W, 256, 0, s>>>(segres, winsum, B / L);
+    msm_window_kernel<<<W, 256, kWindowSmem, s>>>(segres, segsum, winsum, B / L, L);
     nl += 2;
     e = cudaGetLastError();
     if (!wout && e == cudaSuccess) e = horner_on_host(winsum, W, (uint32_t)p.c, d_out, s);
   }
   for (void* ptr : {(void*)counts, (void*)offsets, (void*)cursor, (void*)bsums, (void*)list, (void*)cnt,
                     (void*)cprev, (void*)np, (void*)joff[0], (void*)joff[1], (void*)fin, (void*)buf[0],
-                    (void*)buf[1], (void*)pre, (void*)tot, (void*)tpre, (void*)buckets, (void*)segres,
+                    (void*)buf[1], (void*)pre, (void*)tot, (void*)tpre, (void*)buckets, (void*)segres, (void*)segsum,
                     (void*)nch, (void*)heavy, (void*)heavy_count, (void*)chunk_res,
                     (void*)(wout ? nullptr : winsum), (void*)bases_rp})
     if (ptr) cudaFreeAsync(ptr, s);

@@ -129,15 +129,21 @@ class Server {
       if (!adm_.reserve(bytes)) return ZKGPU_EADMIT;
       peak_ = std::max(peak_, adm_.used() + adm_.reserved());
     }
-    ZK_TRY("cudaSetDevice", cudaSetDevice(device_));
     BaseSet b;
     b.n = n;
-    ZK_TRY("cudaMalloc(bases)", cudaMalloc((void**)&b.d, std::max<uint64_t>(bytes, 64)));
-    ZK_TRY("bases H2D", cudaMemcpy(b.d, xy, bytes, cudaMemcpyHostToDevice));
     // resident bases are kept in the curve arithmetic's R' form: converted
-    // once here instead of on every MSM over them
-    ZK_TRY("bases convert", msm_convert_bases(b.d, b.d, n, s_msm_[0]));
-    ZK_TRY("bases convert sync", cudaStreamSynchronize(s_msm_[0]));
+    // once here (in place) instead of on every MSM over them
+    cudaError_t e = cudaSetDevice(device_);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&b.d, std::max<uint64_t>(bytes, 64));
+    if (e == cudaSuccess) e = cudaMemcpy(b.d, xy, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = msm_convert_bases(b.d, b.d, n, s_msm_[0]);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s_msm_[0]);
+    if (e != cudaSuccess) {
+      if (b.d) cudaFree(b.d);
+      std::lock_guard<std::mutex> lk(mu_);
+      adm_.unreserve(bytes);
+      return status_of("add_bases", e);
+    }
     std::lock_guard<std::mutex> lk(mu_);
     bases_.push_back(b);
     *id = (uint32_t)bases_.size() - 1;
