@@ -351,6 +351,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                 "kernel_ms_per_launch": round(d["ms"] / d["launches"], 4),
                 "peak_source": "measured live: zkgpu_int_peak (mad.lo.cc/madc.hi.cc chains, all SMs)",
                 "modmul_rate_measured_gps": round(modmul_ps / 1e9, 2)}
+        if name in PIPE_FRACS:
+            roof["pipes"] = PIPE_FRACS[name]
 
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "Melem/s", "n_gpus": world, "steps": args.steps,
@@ -922,6 +924,7 @@ def msm_roofline(prof: dict, imad_ps: float, n: int, total_ms: float):
     if b:
         out["bucket_kernel_ms_per_launch"] = round(b["ms"] / b["launches"], 3)
         out["bucket_kernel_share"] = round(b["ms"] / sum(v["ms"] for v in prof.values()), 3)
+    out["pipes"] = PIPE_FRACS["msm_apply"]
     return out
 
 
@@ -933,6 +936,18 @@ HBM_GBS = 6543.1
 TRAFFIC_RATIO = {"ntt_pass_b6": 0.97}
 TRAFFIC_SOURCE = {"ntt_pass_b6": "ncu dram__bytes_read.sum + dram__bytes_write.sum of ntt_pass_kernel<6> on a "
                                  "2^24 transform (plan 6+6+6+6), scaled by algorithmic bytes"}
+# Pipe utilisation of the dominant kernels from one ncu --set full capture
+# each (ntt_pass_kernel<6> on a 2^24 transform, ba_apply_kernel<1> in the
+# 2^22 MSM): the IMAD-convention frac counts products per second, these say
+# how busy the pipes the FP64-limb product actually uses are.
+PIPE_FRACS = {
+    "ntt_pass_b6": {"fp64": 0.367, "alu": 0.482, "fma_imad": 0.052, "issue_active": 0.482, "warps_active": 0.249,
+                    "source": "ncu sm__inst_executed_pipe_{fp64,alu,fma}, smsp__issue_active, sm__warps_active of "
+                              "ntt_pass_kernel<6> on a 2^24 transform (second pass)"},
+    "msm_apply": {"kernel": "ba_apply_kernel<1> (round 0, 54 % of the MSM with the other rounds)",
+                  "fp64": 0.324, "alu": 0.464, "fma_imad": 0.074, "issue_active": 0.492, "warps_active": 0.240,
+                  "source": "ncu --set full of ba_apply_kernel<1> in the 2^22 MSM"},
+}
 
 
 def _load_peaks():
