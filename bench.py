@@ -170,6 +170,21 @@ def cpu_lde_sample(k: int = LOG_N, e: int = LOG_EXT - LOG_N, seed: int = 5):
     return time.perf_counter() - t0, threads
 
 
+def cpu_ntt16_ms(calls: int = 20) -> tuple:
+    """The single forward NTT 2^16 on the host (oracle restatement of halo2
+    best_fft, OpenMP on all host threads): median ms of `calls` calls."""
+    from oracle import pyoracle as O
+    threads = os.cpu_count() or 1
+    a = rand_fr(1 << 16, 1616)
+    w = mont(root_of_unity(16))
+    ts = []
+    for _ in range(calls):
+        t0 = time.perf_counter()
+        O.best_fft(a, w, 16, threads)
+        ts.append(time.perf_counter() - t0)
+    return float(np.median(ts)) * 1e3, threads
+
+
 def lde_work(k: int, e: int) -> float:
     """algorithmic Fr products of the LDE (radix-2 convention)"""
     return (2**k / 2) * k + 2**k + 2**k + (2 ** (k + e) / 2) * (k + e)
@@ -304,6 +319,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     stream.synchronize()
     ntt_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
     del d_a
+    ntt16 = bench_ntt16(zk, torch, dev, stream)
 
     # ---- MSM 2^22 (sub-metric): 10% of scalars < 2^16, resident bases ----
     n_msm = 1 << 22
@@ -364,6 +380,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "kernels": {k: {"launches": v["launches"], "ms": round(v["ms"], 3)} for k, v in prof.items()},
         "extra": {"ntt_fwd_2p24_melem_s": round(world * n / (ntt_ms * 1e-3) / 1e6, 2),
                   "ntt_fwd_2p24_ms": round(ntt_ms, 4),
+                  "ntt_fwd_2p16": ntt16,
                   "msm_2p22_mpts_s": round(world * n_msm / (msm_ms * 1e-3) / 1e6, 2),
                   "msm_2p22_ms": round(msm_ms, 3),
                   "msm_inputs": "bases k_i*(1,2) for seeded uniform Fr k_i (device fixed-base multiplication); "
@@ -376,9 +393,11 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         t, threads = cpu_lde_sample()
+        t16, _ = cpu_ntt16_ms()
         line["cpu_baseline"] = {"value": round(cpu_melem_s(t), 3), "unit": "Melem/s", "cores": threads,
                                 "kind": "port",
-                                "sample": "one full halo2 LDE 2^24 -> 2^26 (oracle port, OpenMP on all host threads)"}
+                                "sample": "one full halo2 LDE 2^24 -> 2^26 (oracle port, OpenMP on all host threads)",
+                                "ntt_fwd_2p16_ms": round(t16, 3)}
     if rank == 0:
         print(json.dumps(line), flush=True)
     group.barrier()
@@ -465,6 +484,47 @@ def bench_e2e(zk, torch, dev: int, vals_np, c, n: int, N: int, steps: int, barri
             "callers": callers, "steps_per_caller": steps_each,
             "single_caller": {"value": round(one_value, 3), "ms_per_step": round(t_one / steps_each * 1e3, 2)},
             "pageable_single_caller": {"value": round(pg_value, 3), "ms_per_step": round(t_pg / pg_steps * 1e3, 2)},
+            "outputs_agree": bool(ok)}
+
+
+def bench_ntt16(zk, torch, dev: int, stream, reps: int = 200, calls: int = 50):
+    """The single forward NTT of 2^16 elements (seeded uniform Fr): device
+    time per call over back-to-back calls (input and tables stay in L2: 2 MiB
+    of data), and the end-to-end time of the reference's own entry point
+    `parallel_fft_api` on a pageable host array (copies in and out inside),
+    median of `calls` calls, checked against the device call's output."""
+    k, n = 16, 1 << 16
+    omega = mont(root_of_unity(k))
+    a = rand_fr(n, 1616)
+    d = torch.from_numpy(a.view(np.int64)).to(f"cuda:{dev}")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    for _ in range(3):
+        zk.ntt_dev(d, k, omega, stream=stream)
+    stream.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        zk.ntt_dev(d, k, omega, stream=stream)
+    e1.record(stream)
+    stream.synchronize()
+    dev_ms = e0.elapsed_time(e1) / reps
+    ref = torch.from_numpy(a.view(np.int64)).to(f"cuda:{dev}")
+    zk.ntt_dev(ref, k, omega, stream=stream)
+    stream.synchronize()
+    ref = ref.cpu().numpy().view(np.uint64)
+    times, ok = [], True
+    for i in range(calls + 3):
+        buf = a.copy()
+        t0 = time.perf_counter()
+        st = zk.parallel_fft_api(dev, buf, omega, None, n, k, 0)
+        dt = time.perf_counter() - t0
+        ok = ok and st == 0 and np.array_equal(buf, ref)
+        if i >= 3:
+            times.append(dt)
+    host_ms = float(np.median(times)) * 1e3
+    return {"device_ms": round(dev_ms, 4), "device_melem_s": round(n / (dev_ms * 1e-3) / 1e6, 1),
+            "parallel_fft_api_ms": round(host_ms, 4), "parallel_fft_api_melem_s": round(n / (host_ms * 1e-3) / 1e6, 1),
+            "host_buffer": "pageable numpy array, in place (the reference's callers pass a Vec)",
             "outputs_agree": bool(ok)}
 
 
