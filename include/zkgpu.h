@@ -288,7 +288,9 @@ void zkgpu_server_destroy(void *server);
  * Diagnostics.
  * ====================================================================== */
 /* elementwise field op on host arrays through the device kernels:
- * op 0 = mul, 1 = add, 2 = sub;  fid 0 = Fr, 1 = Fq */
+ * op 0 = mul, 1 = add, 2 = sub (Montgomery form);  fid 0 = Fr, 1 = Fq;
+ * op 3 (Fq only, b unused and may be null) = the inverse of plain canonical
+ * integers a < q, 0 for 0: the MSM rounds' divstep inversion */
 int zkgpu_field_op(int device, int op, int fid, const uint64_t *a, const uint64_t *b, uint64_t *out, uint64_t n);
 /* failure detection: runs a batch whose dependency wait can never be met;
  * the kernel gives up after about spin_us and the call returns

@@ -25,3 +25,19 @@ def test_divstep_inversion_matches_bigint(tmp_path):
     assert len(out) == len(vals)
     for v, r in zip(vals, out):
         assert int(r, 16) == pow(v, -1, Q), hex(v)
+
+
+@pytest.mark.gpu
+def test_device_divstep_inversion_matches_bigint(zk):
+    """The same inversion on the GPU (zkgpu_field_op op 3, the function the
+    MSM rounds call): edges, long runs of equal bits and random values."""
+    import numpy as np
+    rng = random.Random(4049)
+    vals = [0, 1, 2, 3, (Q - 1) // 2, Q - 2, Q - 1] + [1 << k for k in range(254)] + \
+        [(1 << k) - 1 for k in range(2, 254)] + [Q - (1 << k) for k in range(253)] + \
+        [rng.randrange(1, Q) for _ in range(8000)]
+    a = np.array([[(v >> (64 * i)) & ((1 << 64) - 1) for i in range(4)] for v in vals], dtype=np.uint64)
+    out = zk.field_op("inv", a, a, "fq")
+    for v, row in zip(vals, out):
+        got = sum(int(w) << (64 * i) for i, w in enumerate(row))
+        assert got == (pow(v, -1, Q) if v else 0), hex(v)

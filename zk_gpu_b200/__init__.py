@@ -234,7 +234,7 @@ def msm(scalars: np.ndarray, bases: np.ndarray, device: int = 0) -> np.ndarray:
 def field_op(op: str, a: np.ndarray, b: np.ndarray, field: str = "fr", device: int = 0) -> np.ndarray:
     a, b = _arr(a), _arr(b)
     out = np.empty_like(a)
-    _check(lib().zkgpu_field_op(device, {"mul": 0, "add": 1, "sub": 2}[op], {"fr": 0, "fq": 1}[field],
+    _check(lib().zkgpu_field_op(device, {"mul": 0, "add": 1, "sub": 2, "inv": 3}[op], {"fr": 0, "fq": 1}[field],
                                 a.ctypes.data, b.ctypes.data, out.ctypes.data, a.shape[0]), "field_op")
     return out
 

@@ -2,6 +2,7 @@
 // field diagnostics (declared in include/zkgpu.h).
 #include <cstring>
 
+#include "fq_inv.cuh"
 #include "ntt.cuh"
 #include "runtime.cuh"
 
@@ -362,15 +363,19 @@ __global__ void field_op_kernel(int op, const fe* a, const fe* b, fe* out, uint6
     zk::mul<P>(r, x, y);
   else if (op == 1)
     zk::add<P>(r, x, y);
-  else
+  else if (op == 2)
     zk::sub<P>(r, x, y);
+  else
+    zk::fq_inv_divsteps(r, x);  // op 3, Fq only (checked on the host): the MSM rounds' inversion
   zk::st_fe(out + i, r);
 }
 }  // namespace
 
 extern "C" int zkgpu_field_op(int device, int op, int fid, const uint64_t* a, const uint64_t* b, uint64_t* out,
                               uint64_t n) {
-  if (!a || !b || !out || op < 0 || op > 2 || fid < 0 || fid > 1) return ZKGPU_EINVAL;
+  if (!a || (op != 3 && !b) || !out || op < 0 || op > 3 || fid < 0 || fid > 1 || (op == 3 && fid != 1))
+    return ZKGPU_EINVAL;
+  if (op == 3) b = a;  // unused operand
   if (n == 0) return ZKGPU_OK;
   cudaStream_t s;
   int st = zk::bind_device(device, &s);
