@@ -259,6 +259,10 @@ typedef struct {
     uint64_t pending, inflight;
     uint64_t msm_merged_passes; /* multi-MSM passes (MSMs of one wave on shared bases) */
     uint64_t msm_merged_jobs;   /* MSM jobs that ran inside such passes */
+    uint64_t table_builds;      /* NTT / coset tables built on this device since the server started (cache misses) */
+    uint64_t cache_clears;      /* table caches dropped by the scheduler to make room (nothing in flight) */
+    uint64_t memory_waits;      /* admission rounds that waited for a wave to retire (head job did not fit) */
+    uint64_t max_launch_us;     /* longest host time the scheduler spent enqueueing one wave */
 } zkgpu_server_stats;
 
 /* device memory a job needs while in flight (bytes) */

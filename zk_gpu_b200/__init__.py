@@ -408,7 +408,8 @@ class Job(ctypes.Structure):
 class ServerStats(ctypes.Structure):
     _fields_ = [(k, ctypes.c_uint64) for k in ("submitted", "rejected", "completed", "failed", "waves",
                                                "batch_launches", "hbm_budget", "hbm_used", "hbm_peak", "pending",
-                                               "inflight", "msm_merged_passes", "msm_merged_jobs")]
+                                               "inflight", "msm_merged_passes", "msm_merged_jobs", "table_builds",
+                                               "cache_clears", "memory_waits", "max_launch_us")]
 
 
 def _set4(dst, v):

@@ -89,6 +89,7 @@ PowTablesRef pow_tables_get(int device, const host::Fr& c, int log_n, cudaStream
 // Bytes the device's table caches hold, and dropping every cached entry
 // (entries still held by work stay alive until it lets go).
 uint64_t table_cache_bytes(int device);
+uint64_t table_cache_builds(int device);  // tables built so far on `device` (cache misses)
 void table_cache_clear(int device);
 
 // Parameters of one pass launch (kernel argument / batch descriptor).

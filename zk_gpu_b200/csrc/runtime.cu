@@ -53,6 +53,18 @@ cudaError_t dmalloc(void** ptr, size_t bytes, cudaStream_t s) {
   return cudaMallocFromPoolAsync(ptr, bytes, pool, s);
 }
 
+cudaError_t reserve_pool(size_t bytes, cudaStream_t s) {
+  void* p = nullptr;
+  cudaError_t e = dmalloc(&p, bytes, s);
+  if (e != cudaSuccess) {
+    cudaGetLastError();  // a failed reservation is not an error of the caller's next call
+    return e;
+  }
+  e = cudaFreeAsync(p, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  return e;
+}
+
 cudaError_t trim_pool(int device) {
   cudaMemPool_t pool = nullptr;
   {

@@ -30,6 +30,12 @@ int bind_device(int device, cudaStream_t* stream);
 // own allocations may use, is left as the caller configured it.  Free with
 // cudaFreeAsync.  zkgpu_release_cached returns the cached memory.
 cudaError_t dmalloc(void** ptr, size_t bytes, cudaStream_t s);
+// Take `bytes` of device memory into the library pool of the current device
+// and keep it there (one block allocated and freed on `s`, then waited for):
+// later allocations are carved from retained memory instead of growing the
+// pool, which maps new memory on the calling thread (30-135 ms for a 3-6 GB
+// request on B200).
+cudaError_t reserve_pool(size_t bytes, cudaStream_t s);
 // Return the library pool's cached, unused memory on `device` to the system.
 cudaError_t trim_pool(int device);
 // Copies for the host-buffer entry points, enqueued on `s`.  Pinned host

@@ -67,6 +67,7 @@ struct Wave {
   std::vector<BatchPass> passes;  // host copy kept alive for the async upload
   std::vector<std::shared_ptr<const void>> tables;  // tables the wave's passes read, held until it retires
   uint64_t* mailbox = nullptr;    // pinned: [0] batch error flag, then kMsmSlotWords per MSM job
+  BatchPass* pass_stage = nullptr;  // pinned upload buffer of this wave's stream slot (kPassStage entries)
   uint64_t extra_bytes = 0;       // budget taken beyond the jobs' footprints (merged MSM passes)
   int status = ZKGPU_OK;
 };
@@ -93,11 +94,28 @@ class Server {
       ZK_TRY("cudaStreamCreate", cudaStreamCreateWithFlags(&s_msm_[i], cudaStreamNonBlocking));
     }
     grid_ = ntt_batch_grid(device_);
+    // take the budget's memory into the library pool now, capped by what the
+    // device has free less a margin for the process's other allocations:
+    // waves then carve their buffers from retained memory instead of growing
+    // the pool while the GPU waits (measured on B200: growing it for a merged
+    // MSM pass's 3-6 GB round buffer held the scheduler 30-135 ms per
+    // allocation, and a few in a row left the GPU idle for up to 3 s).  A
+    // reservation that fails leaves the pool to grow on demand.
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+      const uint64_t margin = 4ull << 30;
+      const uint64_t want = std::min<uint64_t>(adm_.budget(), free_b > margin ? free_b - margin : 0);
+      if (want >= (1ull << 30)) reserve_pool(want, s_ntt_[0]);
+    }
     // one pinned mailbox per stream slot; a slot is reused only after the
     // wave that used it retired (waves retire in launch order)
     // per job: an MSM slot, plus room for the multi-MSM offsets (one word)
     slot_words_ = 2 + (kMsmSlotWords + 1) * (uint64_t)max_wave_ + 2;
     ZK_TRY("cudaMallocHost(mailbox)", cudaMallocHost((void**)&mailbox_, kStreams * slot_words_ * 8));
+    // the batch pass lists are uploaded from pinned memory: a copy from
+    // pageable memory may make the enqueueing thread wait for the stream
+    ZK_TRY("cudaMallocHost(pass stage)",
+           cudaMallocHost((void**)&pass_stage_, kStreams * kPassStage * sizeof(BatchPass)));
     sched_ = std::thread([this] { sched_loop(); });
     comp_ = std::thread([this] { comp_loop(); });
     return ZKGPU_OK;
@@ -116,6 +134,8 @@ class Server {
     cudaDeviceSynchronize();
     for (auto& b : bases_) cudaFree(b.d);
     if (mailbox_) cudaFreeHost(mailbox_);
+    if (pass_stage_) cudaFreeHost(pass_stage_);
+    trim_pool(device_);  // give back the pool memory nothing holds any more
     for (int i = 0; i < kStreams; i++) {
       if (s_ntt_[i]) cudaStreamDestroy(s_ntt_[i]);
       if (s_msm_[i]) cudaStreamDestroy(s_msm_[i]);
@@ -210,11 +230,18 @@ class Server {
     o->inflight = inflight_jobs_;
     o->msm_merged_passes = merged_passes_;
     o->msm_merged_jobs = merged_jobs_;
+    o->table_builds = table_cache_builds(device_) - builds0_;
+    o->cache_clears = cache_clears_;
+    o->memory_waits = memory_waits_;
+    o->max_launch_us = max_launch_us_;
   }
 
  private:
   static constexpr int kStreams = 8;
   static constexpr int kEagerWaves = kStreams;
+  // pass descriptors a stream slot's pinned upload buffer holds (a 64-job
+  // wave of LDEs needs a few hundred)
+  static constexpr size_t kPassStage = 2048;
   int eager_waves_ = kEagerWaves;
   // per MSM job in a wave's mailbox: window count, c, then the window sums
   static constexpr uint64_t kMsmSlotWords = 2 + 16 * (uint64_t)MSM_MAX_WINDOWS;
@@ -247,11 +274,13 @@ class Server {
           if (waves_inflight_ == 0 && adm_.external() > 0) {
             // nothing will retire to make room: drop the cached tables (work
             // still holding some keeps them alive) and try again
+            cache_clears_++;
             lk.unlock();
             table_cache_clear(device_);
             continue;
           }
           // the head does not fit yet: wait until a wave retires and frees memory
+          memory_waits_++;
           cv_sched_.wait(lk, [&] { return stop_ || retired_gen_ != gen; });
           continue;
         }
@@ -263,10 +292,14 @@ class Server {
       w->s_ntt = s_ntt_[rr];
       w->s_msm = s_msm_[rr];
       w->mailbox = mailbox_ + rr * slot_words_;
+      w->pass_stage = pass_stage_ + (size_t)rr * kPassStage;
       rr = (rr + 1) % kStreams;
+      const auto tl0 = clk::now();
       launch_wave(*w);
+      const uint64_t tl_us = (uint64_t)std::chrono::duration_cast<std::chrono::microseconds>(clk::now() - tl0).count();
       {
         std::lock_guard<std::mutex> lk(mu_);
+        max_launch_us_ = std::max(max_launch_us_, tl_us);
         waves_++;
         inflight_.push_back(std::move(w));
       }
@@ -503,7 +536,7 @@ class Server {
       const size_t np = w.passes.size();
       if (ok(zk::dmalloc((void**)&dp, np * sizeof(BatchPass), w.s_ntt)) &&
           ok(zk::dmalloc((void**)&dc, (2 + np) * 4, w.s_ntt)) &&
-          ok(cudaMemcpyAsync(dp, w.passes.data(), np * sizeof(BatchPass), cudaMemcpyHostToDevice, w.s_ntt)) &&
+          ok(upload_passes(w, dp, np)) &&
           ok(cudaMemsetAsync(dc, 0, (2 + np) * 4, w.s_ntt))) {
         ok(ntt_batch_launch(dp, (uint32_t)np, (uint32_t)tiles, dc, dc + 2, dc + 1, grid_, w.s_ntt));
         ok(cudaMemcpyAsync(w.mailbox, dc + 1, 4, cudaMemcpyDeviceToHost, w.s_ntt));
@@ -538,6 +571,18 @@ class Server {
     cudaEventRecord(w.ev_ntt, w.s_ntt);
     cudaEventRecord(w.ev_msm, w.s_msm);
     if (e != cudaSuccess) w.status = status_of("server wave", e);
+  }
+
+  // the wave's pass list to device memory, through the slot's pinned buffer
+  // (reused only after the slot's previous wave retired, as the mailbox);
+  // a list longer than the buffer goes from the wave's own copy
+  static cudaError_t upload_passes(Wave& w, BatchPass* dp, size_t np) {
+    const void* src = w.passes.data();
+    if (np <= kPassStage) {
+      std::memcpy(w.pass_stage, w.passes.data(), np * sizeof(BatchPass));
+      src = w.pass_stage;
+    }
+    return cudaMemcpyAsync(dp, src, np * sizeof(BatchPass), cudaMemcpyHostToDevice, w.s_ntt);
   }
 
   // per-job completion event on the stream that produced the job's result
@@ -666,9 +711,12 @@ class Server {
   bool stop_ = false;
   uint64_t next_ticket_ = 1, submitted_ = 0, rejected_ = 0, completed_ = 0, failed_ = 0, waves_ = 0;
   uint64_t batch_launches_ = 0, peak_ = 0, inflight_jobs_ = 0, retired_gen_ = 0;
+  uint64_t cache_clears_ = 0, memory_waits_ = 0, max_launch_us_ = 0;
+  uint64_t builds0_ = table_cache_builds(device_);  // the cache's count when this server started
   std::atomic<uint64_t> merged_passes_{0}, merged_jobs_{0};
   int waves_inflight_ = 0;
   uint64_t* mailbox_ = nullptr;
+  BatchPass* pass_stage_ = nullptr;
   uint64_t slot_words_ = 0;
 };
 

@@ -54,6 +54,7 @@ std::mutex g_mu;
 std::map<NttKey, Entry<NttTables>> g_ntt;
 std::map<PowKey, Entry<PowTables>> g_pow;
 std::map<int, uint64_t> g_bytes;  // per device
+std::map<int, uint64_t> g_builds;  // tables built (misses), per device
 uint64_t g_tick = 0;
 
 uint64_t cap_bytes() {
@@ -134,6 +135,10 @@ NttTablesRef ntt_tables_get(int device, const host::Fr& omega, int log_n, cudaSt
       return it->second.ref;
     }
   }
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_builds[device]++;
+  }
   NttTables* t = new NttTables();
   cudaError_t e = ntt_tables_build(t, plan, omega, s);  // synchronises s
   if (e != cudaSuccess) {
@@ -175,6 +180,10 @@ PowTablesRef pow_tables_get(int device, const host::Fr& c, int log_n, cudaStream
       return it->second.ref;
     }
   }
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_builds[device]++;
+  }
   PowTables* t = new PowTables();
   cudaError_t e = pow_tables_make(t, c, log_n, s, scale, false);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -204,6 +213,12 @@ PowTablesRef pow_tables_get(int device, const host::Fr& c, int log_n, cudaStream
   }
   *err = cudaSuccess;
   return out;
+}
+
+uint64_t table_cache_builds(int device) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  auto it = g_builds.find(device);
+  return it == g_builds.end() ? 0 : it->second;
 }
 
 uint64_t table_cache_bytes(int device) {
