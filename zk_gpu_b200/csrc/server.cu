@@ -135,7 +135,8 @@ class Server {
     for (auto& b : bases_) cudaFree(b.d);
     if (mailbox_) cudaFreeHost(mailbox_);
     if (pass_stage_) cudaFreeHost(pass_stage_);
-    trim_pool(device_);  // give back the pool memory nothing holds any more
+    // the reserved pool memory stays with the library for later calls (as
+    // all pooled memory does); zkgpu_release_cached gives it back
     for (int i = 0; i < kStreams; i++) {
       if (s_ntt_[i]) cudaStreamDestroy(s_ntt_[i]);
       if (s_msm_[i]) cudaStreamDestroy(s_msm_[i]);
