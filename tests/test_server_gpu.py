@@ -84,8 +84,7 @@ def test_server_admission_rejects_and_drains(zk, oracle):
         assert np.array_equal(o, oracle.best_fft(a, oracle.omega(16), 16))
     st = srv.stats()
     assert st["rejected"] == 1 and st["completed"] == 30 and st["hbm_peak"] <= st["hbm_budget"]
-    # the scheduler's own counters: it enqueued waves, and a 64 MiB budget
-    # never had to wait for memory at admission (every job fits alone)
+    # the scheduler's own counters are reported (waves enqueued, timed)
     assert st["max_launch_us"] > 0 and st["waves"] >= 1
     assert st["cache_clears"] >= 0 and st["table_builds"] >= 0
     srv.close()
