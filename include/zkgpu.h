@@ -276,7 +276,10 @@ uint64_t zkgpu_admission_simulate(uint64_t budget, const uint64_t *footprints, u
 /* max_wave_jobs: jobs per scheduling wave (0 = 256); up to 8 waves are on
  * the GPU at once.  The server pins 8 x (32 + 8216 x max_wave_jobs) bytes of
  * host memory for its result mailboxes (an MSM job's window sums come back
- * there; 16.8 MB at 256).
+ * there; 16.8 MB at 256) and 8 x 2048 batch pass descriptors.  At start it
+ * takes hbm_budget_bytes (at most the device's free memory less 4 GB) into
+ * the library's memory pool, where it stays after zkgpu_server_destroy until
+ * zkgpu_release_cached.
  * MSM jobs of one wave against the same bases run as one multi-MSM pass. */
 int zkgpu_server_create(int device, uint64_t hbm_budget_bytes, uint32_t max_wave_jobs, void **server);
 /* upload a base set once (affine, 8 words per point); it stays resident */
