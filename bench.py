@@ -1011,7 +1011,7 @@ HBM_GBS = 6543.1
 # DRAM bytes (read + write) per launch over algorithmic bytes, from one ncu
 # capture of the same kernel on a smaller case (traffic grows with the
 # elements processed): ntt_pass_kernel<6> on a 2^24 transform, plan 6+6+6+6,
-# launches 1.583 / 1.611 GB and 1.034 / 1.082 GB.
+# launches 1.588 / 1.611 GB and 1.051 / 1.082 GB.
 TRAFFIC_RATIO = {"ntt_pass_b6": 0.97}
 TRAFFIC_SOURCE = {"ntt_pass_b6": "ncu dram__bytes_read.sum + dram__bytes_write.sum of ntt_pass_kernel<6> on a "
                                  "2^24 transform (plan 6+6+6+6), scaled by algorithmic bytes"}
@@ -1020,7 +1020,7 @@ TRAFFIC_SOURCE = {"ntt_pass_b6": "ncu dram__bytes_read.sum + dram__bytes_write.s
 # 2^22 MSM): the IMAD-convention frac counts products per second, these say
 # how busy the pipes the FP64-limb product actually uses are.
 PIPE_FRACS = {
-    "ntt_pass_b6": {"fp64": 0.367, "alu": 0.482, "fma_imad": 0.052, "issue_active": 0.482, "warps_active": 0.249,
+    "ntt_pass_b6": {"fp64": 0.398, "alu": 0.525, "fma_imad": 0.097, "issue_active": 0.579, "warps_active": 0.245,
                     "source": "ncu sm__inst_executed_pipe_{fp64,alu,fma}, smsp__issue_active, sm__warps_active of "
                               "ntt_pass_kernel<6> on a 2^24 transform (second pass)"},
     "msm_apply": {"kernel": "ba_apply_kernel<1> (round 0, 54 % of the MSM with the other rounds)",

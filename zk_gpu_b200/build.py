@@ -31,9 +31,9 @@ BUILD = os.environ.get("ZKGPU_BUILD_DIR", BUILD)
 LIB = os.environ.get("ZKGPU_LIB_OUT", LIB)
 
 
-# per-file ptxas options: the wide NTT passes spill far less at -O1 and run
-# faster there (measured on B200; see ntt_tile.cuh)
-FILE_FLAGS = {"ntt_pass_wide.cu": ["-Xptxas", "-O1"]}
+# per-file options (none at present: every NTT pass builds at -O3 since its
+# butterfly products became out-of-line calls; see ntt_tile.cuh)
+FILE_FLAGS: dict = {}
 
 
 def _headers_mtime() -> float:

@@ -1,5 +1,5 @@
-// ntt_pass_wide.cu — launchers of the radix-2^7 .. 2^11 NTT passes, built
-// with their own ptxas options (see ntt_tile.cuh and build.py).
+// ntt_pass_wide.cu — launchers of the radix-2^7 .. 2^11 NTT passes, in a
+// translation unit of their own (see ntt_tile.cuh and build.py).
 #include "ntt_tile.cuh"
 
 namespace zk {

@@ -3,12 +3,12 @@
 // the per-pass kernels, the persistent batch kernel and their launchers.
 //
 // The launchers of the wide passes (B = 7..11) live in their own translation
-// unit, ntt_pass_wide.cu, so that it can be compiled with different ptxas
-// options: at 128 registers per thread (2 CTAs of 256 threads per SM), the
-// three register rounds of a wide pass made ptxas -O3 spill about 1.3 KB per
-// thread with the FP64 product, while -O1 spills about 100 B and runs the
-// 2^26 radix-2^8 pass 22 % faster; the narrow passes (B <= 6, two rounds) are
-// fastest at -O3.
+// unit, ntt_pass_wide.cu, which compiles in parallel with ntt.cu and can take
+// its own ptxas options.  With inlined products, the three register rounds of
+// a wide pass made ptxas -O3 spill about 1.3 KB per thread at 128 registers
+// and -O1 was faster; with the out-of-line products below, -O3 spills
+// 200-380 B and runs the radix-2^8 and 2^9 plans as fast as or faster than
+// -O1, so every pass is built at -O3.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -43,6 +43,72 @@ __device__ __forceinline__ void st_smem_fe(uint32_t* plane0, uint32_t plane_stri
   for (int k = 0; k < 8; k++) plane0[k * plane_stride + a] = r[k];
 }
 
+// The products of a pass.  With ZK_NTT_CALL_PRODUCT (the default) the
+// butterfly products are calls of one out-of-line product, its operands and
+// result passed by value so that they stay in registers: a radix-8 round then
+// runs one product's code from the instruction cache instead of a fresh
+// inlined copy per butterfly, whose cache misses held the fully unrolled
+// rounds back.  The products outside the rounds (the twist, the coset
+// pre-multiply, the output scale) are calls only in passes of width
+// B >= ZK_NTT_CALL_EDGE_MIN_B: inlined they overlap their loads and run
+// faster in the narrow passes, while in the wide ones the shorter code and
+// lower register pressure win (measured on B200, bit-identical results:
+// forward NTT 2^24 of four radix-2^6 passes 4.77 -> 4.46 ms, radix-2^8 plan
+// 5.19 -> 5.15 ms, 512 batched jobs 2^10..2^20 33.0 -> ~29.5 ms, the same
+// jobs one call each 99 -> 69-82 ms).
+#ifndef ZK_NTT_CALL_PRODUCT
+#define ZK_NTT_CALL_PRODUCT 1
+#endif
+#ifndef ZK_NTT_CALL_EDGE_MIN_B
+#define ZK_NTT_CALL_EDGE_MIN_B 7
+#endif
+struct Fe8 { uint32_t w[8]; };
+struct Tw5 { double d[5]; };
+template <class P>
+__device__ __noinline__ Fe8 mul_rp_pre_call(const Fe8 a, const Tw5 b) {
+  Fe8 r;
+  mul_rp_pre<P>(r.w, a.w, b.d);
+  return r;
+}
+template <class P>
+__device__ __noinline__ Fe8 mul_rp_call(const Fe8 a, const Fe8 b) {
+  Fe8 r;
+  mul_rp<P>(r.w, a.w, b.w);
+  return r;
+}
+template <bool CALL = (ZK_NTT_CALL_PRODUCT != 0)>
+__device__ __forceinline__ void ntt_mul(uint32_t r[8], const uint32_t a[8], const uint32_t b[8]) {
+#if ZK_NTT_CALL_PRODUCT
+  if constexpr (!CALL) {
+    mul_rp<P_r>(r, a, b);
+    return;
+  }
+  Fe8 av, bv;
+#pragma unroll
+  for (int k = 0; k < 8; k++) av.w[k] = a[k], bv.w[k] = b[k];
+  const Fe8 rv = mul_rp_call<P_r>(av, bv);
+#pragma unroll
+  for (int k = 0; k < 8; k++) r[k] = rv.w[k];
+#else
+  mul_rp<P_r>(r, a, b);
+#endif
+}
+__device__ __forceinline__ void ntt_mul_pre(uint32_t r[8], const uint32_t a[8], const double w[5]) {
+#if ZK_NTT_CALL_PRODUCT
+  Fe8 av;
+  Tw5 wv;
+#pragma unroll
+  for (int k = 0; k < 8; k++) av.w[k] = a[k];
+#pragma unroll
+  for (int k = 0; k < 5; k++) wv.d[k] = w[k];
+  const Fe8 rv = mul_rp_pre_call<P_r>(av, wv);
+#pragma unroll
+  for (int k = 0; k < 8; k++) r[k] = rv.w[k];
+#else
+  mul_rp_pre<P_r>(r, a, w);
+#endif
+}
+
 // One round: registers hold i(r) = ins3<LO>(q, r); perform the DIF stages
 // with butterfly bits HI-1 .. LO.  tws: inner roots w_m^e (e < m/2), 5 planes.
 template <int B, int LO, int HI>
@@ -67,13 +133,13 @@ __device__ __forceinline__ void ntt_round(uint32_t x[8][8], uint32_t q, const do
         } else {
           double w[5];
           ld_smem_tw(w, tws, HALF, e);
-          mul_rp_pre<P_r>(x[r2], t, w);
+          ntt_mul_pre(x[r2], t, w);
         }
       } else {
         const uint32_t e = ((q & ((1u << LO) - 1u)) | ((uint32_t)(r & ((1 << rb) - 1)) << LO)) << (B - 1 - b);
         double w[5];
         ld_smem_tw(w, tws, HALF, e);
-        mul_rp_pre<P_r>(x[r2], t, w);
+        ntt_mul_pre(x[r2], t, w);
       }
     }
   }
@@ -181,8 +247,8 @@ __device__ __forceinline__ void ntt_pass_tile(const PassParams& p, uint64_t tile
       uint32_t a[8], b[8];
       ld_fe_nc(a, p.pre_lo + (xi & mask));
       ld_fe_nc(b, p.pre_hi + (xi >> p.pre_shift));
-      mul_rp<P_r>(a, a, b);
-      mul_rp<P_r>(x[r], x[r], a);
+      ntt_mul<(B >= ZK_NTT_CALL_EDGE_MIN_B)>(a, a, b);
+      ntt_mul<(B >= ZK_NTT_CALL_EDGE_MIN_B)>(x[r], x[r], a);
     }
   }
   __syncthreads();
@@ -198,7 +264,7 @@ __device__ __forceinline__ void ntt_pass_tile(const PassParams& p, uint64_t tile
       uint32_t w[8];
       const uint32_t kj = (k << p.log_J) + col;
       ld_fe_nc(w, p.twist + kj);
-      mul_rp<P_r>(x[r], x[r], w);
+      ntt_mul<(B >= ZK_NTT_CALL_EDGE_MIN_B)>(x[r], x[r], w);
       st_fe(p.out + (((o << B) << p.log_J) + kj), x[r]);
     }
   } else {
@@ -228,11 +294,11 @@ __device__ __forceinline__ void ntt_pass_tile(const PassParams& p, uint64_t tile
         uint32_t a[8], b[8];
         ld_fe_nc(a, p.post_lo + (kout & ((1u << p.post_shift) - 1u)));
         ld_fe_nc(b, p.post_hi + (kout >> p.post_shift));
-        mul_rp<P_r>(a, a, b);
-        mul_rp<P_r>(v, x[r], a);
+        ntt_mul<(B >= ZK_NTT_CALL_EDGE_MIN_B)>(a, a, b);
+        ntt_mul<(B >= ZK_NTT_CALL_EDGE_MIN_B)>(v, x[r], a);
         reduce_once<P_r>(v, v);
       } else if (p.has_post) {
-        mul_rp<P_r>(v, x[r], p.post.w);
+        ntt_mul<(B >= ZK_NTT_CALL_EDGE_MIN_B)>(v, x[r], p.post.w);
         reduce_once<P_r>(v, v);
       } else {
         reduce_once<P_r>(v, x[r]);
