@@ -1023,9 +1023,10 @@ PIPE_FRACS = {
     "ntt_pass_b6": {"fp64": 0.398, "alu": 0.525, "fma_imad": 0.097, "issue_active": 0.579, "warps_active": 0.245,
                     "source": "ncu sm__inst_executed_pipe_{fp64,alu,fma}, smsp__issue_active, sm__warps_active of "
                               "ntt_pass_kernel<6> on a 2^24 transform (second pass)"},
-    "msm_apply": {"kernel": "ba_apply_kernel<1> (round 0, 54 % of the MSM with the other rounds)",
-                  "fp64": 0.324, "alu": 0.464, "fma_imad": 0.074, "issue_active": 0.492, "warps_active": 0.240,
-                  "source": "ncu --set full of ba_apply_kernel<1> in the 2^22 MSM"},
+    "msm_apply": {"kernel": "ba_apply_kernel<1> (round 0, 55 % of the MSM with the other rounds)",
+                  "fp64": 0.350, "alu": 0.504, "fma_imad": 0.105, "issue_active": None, "warps_active": 0.238,
+                  "source": "ncu sections SpeedOfLight, WarpStateStats, ComputeWorkloadAnalysis and LaunchStats "
+                            "of ba_apply_kernel<1> in the 2^22 MSM (issue active not in those sections)"},
 }
 
 

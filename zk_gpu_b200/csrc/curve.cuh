@@ -29,8 +29,34 @@ struct aff_t {
 };
 
 // ---- lazy R'-form Fq helpers --------------------------------------------
-__device__ __forceinline__ void qmul(uint32_t r[8], const uint32_t a[8], const uint32_t b[8]) { mul_rp<P_q>(r, a, b); }
-__device__ __forceinline__ void qsqr(uint32_t r[8], const uint32_t a[8]) { mul_rp<P_q>(r, a, a); }
+// ZK_MSM_CALL_PRODUCT: 0 = every product inlined; 1 = only the products of
+// the batch-affine apply pass (qmul_c / qsqr_c) are calls of one out-of-line
+// product (mul_rp_out); 2 (the default) = every qmul / qsqr is such a call.
+// Measured on B200 with bit-identical outputs, MSM of 2^22 / 2^20 / 2^18 /
+// 2^16 points: inlined 14.85 / 5.77 / 3.14 / 2.01 ms, apply pass only
+// 14.8 / 5.8 / 3.1 / 2.0 ms, every product 14.42 / 5.32 / 2.75 / 1.82 ms:
+// the XYZZ reduction and tail kernels, which inline a dozen or more products
+// per thread, lose their spills (112 B -> 0 in the window kernel at 255
+// registers) and their instruction-cache misses.
+#ifndef ZK_MSM_CALL_PRODUCT
+#define ZK_MSM_CALL_PRODUCT 2
+#endif
+__device__ __forceinline__ void qmul(uint32_t r[8], const uint32_t a[8], const uint32_t b[8]) {
+#if ZK_MSM_CALL_PRODUCT >= 2
+  mul_rp_out<P_q>(r, a, b);
+#else
+  mul_rp<P_q>(r, a, b);
+#endif
+}
+__device__ __forceinline__ void qsqr(uint32_t r[8], const uint32_t a[8]) { qmul(r, a, a); }
+__device__ __forceinline__ void qmul_c(uint32_t r[8], const uint32_t a[8], const uint32_t b[8]) {
+#if ZK_MSM_CALL_PRODUCT >= 1
+  mul_rp_out<P_q>(r, a, b);
+#else
+  mul_rp<P_q>(r, a, b);
+#endif
+}
+__device__ __forceinline__ void qsqr_c(uint32_t r[8], const uint32_t a[8]) { qmul_c(r, a, a); }
 __device__ __forceinline__ void qadd(uint32_t r[8], const uint32_t a[8], const uint32_t b[8]) { add_lazy<P_q>(r, a, b); }
 __device__ __forceinline__ void qsub(uint32_t r[8], const uint32_t a[8], const uint32_t b[8]) { sub_lazy<P_q>(r, a, b); }
 __device__ __forceinline__ void qdbl(uint32_t r[8], const uint32_t a[8]) { add_lazy<P_q>(r, a, a); }

@@ -625,6 +625,28 @@ __device__ __forceinline__ void mul_rp_pre(uint32_t r[8], const uint32_t a[8], c
   mul52_cols<P>(rl, al, bl);
   pack52(r, rl);
 }
+// The same product as a call of one out-of-line function: operands and
+// result pass by value (in registers), so a kernel that runs many products
+// keeps one copy of the product's ~360 instructions in the instruction cache
+// instead of one inlined copy per call site.
+struct Fe8 {
+  uint32_t w[8];
+};
+template <class P>
+__device__ __noinline__ Fe8 mul_rp_call(const Fe8 a, const Fe8 b) {
+  Fe8 r;
+  mul_rp<P>(r.w, a.w, b.w);
+  return r;
+}
+template <class P>
+__device__ __forceinline__ void mul_rp_out(uint32_t r[8], const uint32_t a[8], const uint32_t b[8]) {
+  Fe8 av, bv;
+#pragma unroll
+  for (int k = 0; k < 8; k++) av.w[k] = a[k], bv.w[k] = b[k];
+  const Fe8 rv = mul_rp_call<P>(av, bv);
+#pragma unroll
+  for (int k = 0; k < 8; k++) r[k] = rv.w[k];
+}
 template <class P>
 __device__ __forceinline__ void set_one_rp(uint32_t r[8]) {
   r[0] = P::D0; r[1] = P::D1; r[2] = P::D2; r[3] = P::D3;

@@ -543,8 +543,8 @@ __global__ void __launch_bounds__(256, 2) ba_apply_kernel(const fe* __restrict__
       if (q > q0) {
         uint32_t p[8];
         sm_fe(p, st, bd, 8);
-        qmul(inv_d, inv_run, p);
-        qmul(inv_run, inv_run, d);
+        qmul_c(inv_d, inv_run, p);
+        qmul_c(inv_run, inv_run, d);
       } else {
         cpy(inv_d, inv_run);
       }
@@ -560,18 +560,18 @@ __global__ void __launch_bounds__(256, 2) ba_apply_kernel(const fe* __restrict__
         if (kind == 1) {
           sub<FqP>(t1, Q.y, P.y);
         } else {  // doubling: 3 x^2 / (2 y)
-          qsqr(t1, P.x);
+          qsqr_c(t1, P.x);
           uint32_t t2[8];
           add_lazy<FqP>(t2, t1, t1);
           add_lazy<FqP>(t1, t2, t1);
         }
-        qmul(lam, t1, inv_d);
-        qsqr(t1, lam);
+        qmul_c(lam, t1, inv_d);
+        qsqr_c(t1, lam);
         qsub(t1, t1, P.x);
         qsub(out.x, t1, Q.x);  // Q.x = P.x when doubling
         reduce_once<FqP>(out.x, out.x);
         qsub(t1, P.x, out.x);
-        qmul(t1, lam, t1);
+        qmul_c(t1, lam, t1);
         qsub(out.y, t1, P.y);
         reduce_once<FqP>(out.y, out.y);
       }

@@ -62,18 +62,11 @@ __device__ __forceinline__ void st_smem_fe(uint32_t* plane0, uint32_t plane_stri
 #ifndef ZK_NTT_CALL_EDGE_MIN_B
 #define ZK_NTT_CALL_EDGE_MIN_B 7
 #endif
-struct Fe8 { uint32_t w[8]; };
 struct Tw5 { double d[5]; };
 template <class P>
 __device__ __noinline__ Fe8 mul_rp_pre_call(const Fe8 a, const Tw5 b) {
   Fe8 r;
   mul_rp_pre<P>(r.w, a.w, b.d);
-  return r;
-}
-template <class P>
-__device__ __noinline__ Fe8 mul_rp_call(const Fe8 a, const Fe8 b) {
-  Fe8 r;
-  mul_rp<P>(r.w, a.w, b.w);
   return r;
 }
 template <bool CALL = (ZK_NTT_CALL_PRODUCT != 0)>
@@ -83,12 +76,7 @@ __device__ __forceinline__ void ntt_mul(uint32_t r[8], const uint32_t a[8], cons
     mul_rp<P_r>(r, a, b);
     return;
   }
-  Fe8 av, bv;
-#pragma unroll
-  for (int k = 0; k < 8; k++) av.w[k] = a[k], bv.w[k] = b[k];
-  const Fe8 rv = mul_rp_call<P_r>(av, bv);
-#pragma unroll
-  for (int k = 0; k < 8; k++) r[k] = rv.w[k];
+  mul_rp_out<P_r>(r, a, b);
 #else
   mul_rp<P_r>(r, a, b);
 #endif
