@@ -52,10 +52,11 @@ __device__ __forceinline__ void st_smem_fe(uint32_t* plane0, uint32_t plane_stri
 // pre-multiply, the output scale) are calls only in passes of width
 // B >= ZK_NTT_CALL_EDGE_MIN_B: inlined they overlap their loads and run
 // faster in the narrow passes, while in the wide ones the shorter code and
-// lower register pressure win (measured on B200, bit-identical results:
-// forward NTT 2^24 of four radix-2^6 passes 4.77 -> 4.46 ms, radix-2^8 plan
-// 5.19 -> 5.15 ms, 512 batched jobs 2^10..2^20 33.0 -> ~29.5 ms, the same
-// jobs one call each 99 -> 69-82 ms).
+// lower register pressure win.  Measured on B200 with bit-identical
+// results, against the build that inlined every product (bench, autotuned
+// plans): forward NTT 2^24 4.72 -> 4.45 ms, LDE 2^24 -> 2^26 25.9 -> 24.7 ms,
+// 512 batched jobs of 2^10..2^20 31.8 -> 28.2 ms, the same jobs one call
+// each 94 -> 71 ms.
 #ifndef ZK_NTT_CALL_PRODUCT
 #define ZK_NTT_CALL_PRODUCT 1
 #endif
