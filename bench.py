@@ -622,6 +622,14 @@ def bench_batched(zk, torch, dev: int, stream, steps: int, njobs: int = 512, see
             "inputs": "uniform 252-bit values (< r) from torch.randint on the device"}
 
 
+def median_closed_run(run, njobs: int, reps: int = 3):
+    """Run a closed loop `reps` times (`run(None)` -> (latencies, span_s));
+    return the median run by span and every run's rate in jobs/s, fastest
+    first."""
+    runs = sorted((run(None) for _ in range(reps)), key=lambda r: r[1])
+    return runs[len(runs) // 2], [round(njobs / r[1], 1) for r in runs]
+
+
 def serving_trace(njobs: int, seed: int = 99):
     """(arrival at rate 1, kind, log_size) per job: Poisson arrivals
     (divide the times by the offered rate); 70% NTT / coset LDE (log2 size
@@ -793,14 +801,10 @@ def bench_serving(zk, torch, dev: int, njobs: int = 1000, rate: float = 2000.0, 
     # closed loops: three runs per arm, the median run (by span) reported and
     # every run's rate listed, so that one run caught by a host-side stall
     # does not set the saturation figures or the one-call capacity
-    def closed_median(run):
-        runs = sorted((run(None) for _ in range(3)), key=lambda r: r[1])
-        return runs[1], [round(n / r[1], 1) for r in runs]
-
     lat_s, span_s = run_server(rate)
-    (lat_sc, span_sc), sc_runs = closed_median(run_server)
+    (lat_sc, span_sc), sc_runs = median_closed_run(run_server, n)
     lat_p, span_p = run_plain(rate)
-    (lat_pc, span_pc), pc_runs = closed_median(run_plain)
+    (lat_pc, span_pc), pc_runs = median_closed_run(run_plain, n)
     st = srv.stats()
     one_cap = n / span_pc
     # ---- equal p99: each arm's p99 latency over a sweep of offered rates on
